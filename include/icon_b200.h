@@ -1,0 +1,147 @@
+/*
+ * icon_b200.h -- C ABI of the B200 ICON reconstruction engine.
+ *
+ * Replaces the internal API of ICON-GPU v1.2.9 (hilbertsun/feilab,
+ * tomography/ICON_GPU_v1.2.9/sourceCode/ICON-GPU; NU = nufft_gpu_v8.cu):
+ * the reference's routines return void, take plan structs by value, run on
+ * the default stream and handle one slice at a time.  Here every call
+ * returns an icon_status, plans are opaque handles, work is queued on the
+ * caller's stream, and every call processes a batch of S slices of one tilt
+ * series (the slices share geometry, which is what makes batching pay).
+ *
+ * Data layout (all arrays are caller-owned unless stated otherwise):
+ *   image   [S][N0][N1]   N0 = detector width nx, N1 = thickness, the
+ *                         thickness index fastest -- the reference's device
+ *                         layout of m, fhat and Ahwb (NU:763-771, :1111-1115)
+ *   nodes   [S][M][2]     M = nx*ntilt complex values, node j = tilt*nx + k
+ *                         (px2D.cu:29-47, readSlicePart.cu:21)
+ *   rows    [S][ntilt][nx] projection rows: row y of every tilt, per slice y
+ *                         (mrc_read_slice(..., 'y', ...), mrcfile3.c:902-951)
+ * Pointers named d_* are device pointers on the plan's device; h_* are host
+ * pointers.  `stream` is a cudaStream_t passed as void* (NULL = the legacy
+ * default stream).  No call synchronises the device except where noted.
+ *
+ * Errors: a non-zero icon_status; icon_last_error() returns a message for the
+ * calling thread.  Nothing here calls exit().
+ * Threading: a plan may be used by one host thread at a time; different plans
+ * are independent.
+ */
+#ifndef ICON_B200_H
+#define ICON_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    ICON_OK = 0,
+    ICON_ERR_INVALID = 1,   /* bad argument or unsupported size            */
+    ICON_ERR_CUDA = 2,      /* a CUDA runtime call failed                  */
+    ICON_ERR_NOMEM = 3,     /* device or host allocation failed            */
+    ICON_ERR_CAPACITY = 4,  /* S larger than the plan's batch capacity     */
+    ICON_ERR_IO = 5,        /* file could not be read or written           */
+    ICON_ERR_TIMEOUT = 6    /* a bounded device-side wait ran out          */
+} icon_status;
+
+typedef struct icon_plan icon_plan;
+
+/* Geometry of one tilt series.  Replaces the set-up of Lib_2D2
+ * (MainCode.cu:12-109): .tlt angles, px2D nodes, Weight(), grid sizes
+ * n_d = 2*nextpow2(N_d), the Gaussian window of half-width 6 and its
+ * deapodisation, cunfft_initPlan_1d / cunfft_initPlan_2d2 (NU:445-556,
+ * NU:1298-1391) and initGICONPara2 (NU:1739-1771). */
+typedef struct {
+    int nx;                  /* detector width, N0 (>= 8)                        */
+    int thickness;           /* N1 (>= 8); 0 means nx, as MainCode.cu:14-16     */
+    int ntilt;               /* number of tilts (>= 2)                            */
+    const float *tilt_deg;   /* h_: angles as written in the .tlt file; they are
+                                negated internally as MainCode.cu:42 does          */
+    int capacity;            /* most slices any single call will pass            */
+    int device;              /* CUDA device ordinal; -1 = the current device     */
+} icon_geometry;
+
+/* Iteration schedule and constraint of Iteration3 (Iteration2.cu:3-150):
+ * `infr_before` unconstrained steps, `icon` clamped steps, `infr_after`
+ * unconstrained steps (the -iter a,b,c flag of ICONGPU.cu:203-211).
+ * data_type 1 clamps m <= threshold, 2 clamps m >= threshold
+ * (ICONUpdateCU_R, NU:1597-1616). */
+typedef struct {
+    int infr_before;
+    int icon;
+    int infr_after;
+    int data_type;
+    float threshold;
+} icon_solve_cfg;
+
+/* icon_plan_create: builds the plan, its device tables and scratch for up to
+ * geo->capacity slices.  Replaces cunfft_mallocPlan_2d2 + cunfft_initPlan_2d2
+ * (NU:281-324, NU:445-556), cunfft_initPlan_1d (NU:1298-1391) and
+ * initGICONPara2 (NU:1739-1771).  Synchronises the device. */
+icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out);
+
+/* Frees a plan (cunfft_destroyPlan_2d2 NU:594-628, cunfft_destroyPlan_1d
+ * NU:1393-1408, destroyGICONPara NU:1774-1787).  Synchronises the device. */
+icon_status icon_plan_destroy(icon_plan *plan);
+
+/* dims[0..9] = N0, N1, n0, n1, M, ntilt, slices per group B, capacity,
+ * device bytes held by the plan (low 31 bits in MiB), tilt index of the
+ * smallest |angle| (the reprojection tilt of MainCode.cu:46-49). */
+icon_status icon_plan_query(const icon_plan *plan, int *dims);
+
+/* h_w[M] <- density weights, h_xy[2M] <- node coordinates (x0, x1), exactly
+ * as Weight() and px2D() compute them (weight.cu:8-41, px2D.cu:8-47).
+ * Either pointer may be NULL. */
+icon_status icon_plan_geometry(const icon_plan *plan, float *h_xy, float *h_w);
+
+/* Forward 2-D NUFFT of real images: d_nodes = A d_img.
+ * Replaces cunfft_trafo_2d_R2C2 (NU:984-1076). */
+icon_status icon_nufft_forward(icon_plan *plan, const float *d_img, void *d_nodes, int S, void *stream);
+
+/* Forward 2-D NUFFT of complex images (cunfft_trafo_2d2, NU:844-949). */
+icon_status icon_nufft_forward_complex(icon_plan *plan, const void *d_img, void *d_nodes, int S, void *stream);
+
+/* Adjoint 2-D NUFFT: d_img (complex) = A^H d_nodes.
+ * Replaces cunfft_adjoint_2d2 (NU:1167-1238). */
+icon_status icon_nufft_adjoint(icon_plan *plan, const void *d_nodes, void *d_img, int S, void *stream);
+
+/* 1-D NUFFT of every projection row: d_b[S][M] complex.
+ * Replaces readSlicePart (readSlicePart.cu:3-31) with cunfft_trafo_1d
+ * (NU:1479-1516) per row. */
+icon_status icon_rows_forward(icon_plan *plan, const float *d_rows, void *d_b, int S, void *stream);
+
+/* Right-hand side A^H W b from projection rows: the input stage of the
+ * slice loop of Lib_2D2 (MainCode.cu:115-134: readSlicePart,
+ * complexMulDoubleCU, cunfft_adjoint_2d2, complexCopyCU). */
+icon_status icon_prepare_rhs(icon_plan *plan, const float *d_rows, void *d_Ahwb, int S, void *stream);
+
+/* ICON iterations on S slices: replaces Iteration3 (Iteration2.cu:3-150)
+ * with Alpha2 (alpha_new2.cu:3-119).  d_m is the start value when
+ * warm_start != 0 and is zeroed first otherwise (Iteration2.cu:33); it
+ * receives the result.  h_alpha and h_rtr, when not NULL, receive the step
+ * length alpha and ||rhat||^2 of every iteration and slice, [iters][S]
+ * (this synchronises the stream at the end). */
+icon_status icon_solve(icon_plan *plan, const icon_solve_cfg *cfg, const void *d_Ahwb, float *d_m, int S,
+                       int warm_start, double *h_alpha, double *h_rtr, void *stream);
+
+/* Reprojection of S solved slices at one tilt angle (given as in the .tlt
+ * file): forward 2-D NUFFT at the nodes of that single tilt, then the 1-D
+ * adjoint NUFFT, real part (reProject_NFFT2, reProject_NFFT.cu:25-42, with
+ * cunfft_adjoint_1d NU:1518-1536).  d_out[S][nx]. */
+icon_status icon_reproject(icon_plan *plan, const float *d_m, float tilt_deg, float *d_out, int S, void *stream);
+
+/* The whole per-slice pipeline of Lib_2D2 (MainCode.cu:113-142) for S
+ * slices from host memory: rows in, reconstructed slices out, plus the
+ * reprojection at the smallest-|angle| tilt when h_reproj is not NULL.
+ * Copies in and out through pinned staging buffers; synchronises. */
+icon_status icon_reconstruct_host(icon_plan *plan, const icon_solve_cfg *cfg, const float *h_rows, float *h_m,
+                                  float *h_reproj, int S);
+
+/* Message for the last failed call on this thread ("" if none). */
+const char *icon_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,103 @@
+"""CPU tests of the oracle: pins it against the reference's own outputs
+(tests/golden, made by tests/golden/make_golden.py from ICON-GPU compiled for
+sm_100a) and against mathematics (direct NDFT, adjoint identity)."""
+import numpy as np
+import pytest
+
+from conftest import min_abs_tilt_index, rel_l2
+from oracle.oracle import OraclePlan, grid_params
+
+# The reference computes in float with cuFFT; these are relative-L2 bounds of
+# oracle vs reference, measured around 2e-7 (stages) and 4e-6 (200 iterations).
+TOL_STAGE = 1e-6
+TOL_SOLVE = 2e-5
+
+
+def test_grid_sizes_match_reference_formula():
+    # n = 2 * nextpow2(N) for every N (MainCode.cu:66-71).
+    for N in list(range(8, 600)) + [1000, 1023, 1024, 1025, 2047, 2048, 4096]:
+        th, n, b, bf = grid_params(N)
+        p2 = 1
+        while p2 < N:
+            p2 *= 2
+        assert n == 2 * p2, N
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_nufft_vs_direct_ndft(prec):
+    tilts = np.arange(-60, 61, 7.5).astype(np.float32)
+    p = OraclePlan(40, 24, tilts, prec)
+    rng = np.random.default_rng(1)
+    img = rng.standard_normal((40, 24))
+    assert rel_l2(p.forward(img), p.ndft_forward(img)) < 5e-6
+    f = rng.standard_normal(p.M) + 1j * rng.standard_normal(p.M)
+    assert rel_l2(p.adjoint(f), p.ndft_adjoint(f)) < 5e-6
+
+
+def test_adjoint_identity_fp64():
+    tilts = np.linspace(-58, 61, 17).astype(np.float32)
+    p = OraclePlan(33, 21, tilts, "f64")
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal((33, 21)) + 1j * rng.standard_normal((33, 21))
+    y = rng.standard_normal(p.M) + 1j * rng.standard_normal(p.M)
+    lhs = np.vdot(y, p.forward(x))
+    rhs = np.vdot(p.adjoint(y), x)
+    assert abs(lhs - rhs) / abs(lhs) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["a", "b", "c", "cli"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_oracle_matches_reference_stages(golden, name, prec):
+    z = golden[name]
+    p = OraclePlan(int(z["nx"]), int(z["thickness"]), z["tilts"], prec)
+    assert rel_l2(p.forward(z["img_r"]), z["ref_fwd_r"]) < TOL_STAGE
+    assert rel_l2(p.forward(z["img_c"]), z["ref_fwd_c"]) < TOL_STAGE
+    assert rel_l2(p.adjoint(z["f"]), z["ref_adj"]) < TOL_STAGE
+    for s in range(int(z["S"])):
+        assert rel_l2(p.rows_forward(z["rows"][s]), z["ref_b"][s]) < TOL_STAGE
+        assert rel_l2(p.rhs(z["rows"][s]), z["ref_Ahwb"][s]) < TOL_STAGE
+
+
+@pytest.mark.parametrize("name", ["a", "b", "cli"])
+def test_oracle_matches_reference_solve(golden, name):
+    z = golden[name]
+    nx, th = int(z["nx"]), int(z["thickness"])
+    p = OraclePlan(nx, th, z["tilts"], "f64")
+    om = float(-z["tilts"][min_abs_tilt_index(z["tilts"])])
+    lp = OraclePlan(nx, th, None, "f64", line_angle=om)
+    a, b, c = [int(v) for v in z["sched"]]
+    for s in range(int(z["S"])):
+        A = p.rhs(z["rows"][s])
+        m = p.solve(A, (a, b, c), int(z["data_type"]), float(z["threshold"]))
+        assert rel_l2(m, z["ref_m"][s]) < TOL_SOLVE
+        assert rel_l2(p.reproject(lp, m), z["ref_reproj"][s]) < TOL_SOLVE
+
+
+def test_oracle_matches_reference_solve_200_iterations(golden):
+    z = golden["c"]
+    p = OraclePlan(int(z["nx"]), int(z["thickness"]), z["tilts"], "f64")
+    A = p.rhs(z["rows"][0])
+    m = p.solve(A, tuple(int(v) for v in z["sched"]), int(z["data_type"]), float(z["threshold"]))
+    assert rel_l2(m, z["ref_m"][0]) < TOL_SOLVE
+
+
+def test_reference_cli_fixture_consistent_with_harness(golden):
+    # The ICON-GPU command-line run and the harness saw the same inputs; the
+    # slice files it wrote hold the harness's m, transposed to X fastest
+    # (saveMRC_real_inv, saveMRC_real.cu:33-56).
+    from feilab_b200 import mrc
+    import io, os, tempfile
+    z = golden["cli"]
+    assert int(z["cli_returncode"]) == 0
+    nx, th = int(z["nx"]), int(z["thickness"])
+    for s in range(int(z["S"])):
+        raw = z[f"cli_mid{s:05d}"].tobytes()
+        with tempfile.NamedTemporaryFile(suffix=".mrc", delete=False) as f:
+            f.write(raw)
+            path = f.name
+        try:
+            h, d = mrc.read(path)
+        finally:
+            os.unlink(path)
+        assert (int(h["nx"]), int(h["ny"]), int(h["nz"]), int(h["mode"])) == (nx, th, 1, 2)
+        np.testing.assert_array_equal(d[0], z["ref_m"][s].T)
