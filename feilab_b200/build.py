@@ -1,0 +1,75 @@
+"""Build recipe of the native library: nvcc for sm_100a, in-tree output.
+
+    python -m feilab_b200.build          # builds feilab_b200/libicon_b200.so
+                                         # and feilab_b200/icon-gpu (CLI)
+
+The library is built in place (next to this file) so it travels with the
+repository; nothing is installed into site-packages.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libicon_b200.so")
+CLI = os.path.join(HERE, "icon-gpu")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
+
+LIB_SOURCES = ["icon_api.cu"]
+LIB_DEPS = ["icon_api.cu", "icon_kernels.cuh", "icon_device.cuh"]
+CLI_SOURCES = ["icon_cli.cpp", "mrc_io.cpp"]
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _nvcc():
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if c and (os.path.sep not in c or os.path.exists(c)):
+            return c
+    return "nvcc"
+
+
+def build_lib(force=False, verbose=False):
+    deps = [os.path.join(CSRC, f) for f in LIB_DEPS] + [os.path.join(ROOT, "include", "icon_b200.h")]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    cmd = [_nvcc(), *ARCH, *NVFLAGS, "-shared", "-o", LIB] + [os.path.join(CSRC, f) for f in LIB_SOURCES]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+def build_cli(force=False, verbose=False):
+    srcs = [os.path.join(CSRC, f) for f in CLI_SOURCES]
+    if not all(os.path.exists(s) for s in srcs):
+        return None
+    deps = srcs + [LIB, os.path.join(CSRC, "mrc_io.h"), os.path.join(ROOT, "include", "icon_b200.h")]
+    if not force and not _stale(CLI, deps):
+        return CLI
+    cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, "-o", CLI, *srcs,
+           "-L" + HERE, "-licon_b200", "-Wl,-rpath,$ORIGIN", "-lpthread"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return CLI
+
+
+def build(force=False, verbose=False):
+    build_lib(force, verbose)
+    build_cli(force, verbose)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

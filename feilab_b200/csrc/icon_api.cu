@@ -1,0 +1,807 @@
+// icon_api.cu -- plans, launch sequences and the C ABI of include/icon_b200.h.
+//
+// Host-side geometry follows the reference exactly (float arithmetic where it
+// uses float); the window tables are evaluated on the device with the same
+// float expressions as nufft_Phi2d_1dCU (NU:221-235), so they carry the same
+// bits as the reference's tables.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "icon_b200.h"
+#include "icon_kernels.cuh"
+
+using icon::Geo;
+using icon::Geo1;
+using icon::kTaps;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+icon_status fail(icon_status st, const std::string &msg)
+{
+    g_last_error = msg;
+    return st;
+}
+
+#define ICON_CUDA(call)                                                                          \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail(ICON_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+
+#define ICON_TRY(expr)                           \
+    do {                                         \
+        icon_status s_ = (expr);                 \
+        if (s_ != ICON_OK) return s_;            \
+    } while (0)
+
+constexpr double kRefPi = 3.1415926535898;      // nufft_gpu_v8.cuh:8
+constexpr double kRefPiPx2d = 3.14159265;       // px2D.cuh:8
+
+// MainCode.cu:66-71 and NU:471-476 (float where the reference stores float).
+void grid_params(int N, float &th, int &n, float &b, float &bf)
+{
+    float uptop = (float)std::pow(2.0, std::ceil(std::log10((double)N) / std::log10(2.0)));
+    th = (float)(2.0 * uptop / (double)N);
+    n = (int)std::ceil(th * (float)N);
+    b = (float)((double)(2 * th * icon::kHalf) / ((double)(2 * th - 1) * kRefPi));
+    bf = (float)(1.0 / std::sqrt(kRefPi * (double)b));
+}
+
+// px2D.cu:8-47: s accumulated in float from -1/2 by 1/nx; x = s*cos, s*sin of
+// angle*pi/180 in double, stored as float.  Output interleaved (x0, x1).
+void px2d(int nx, int nz, const float *th_neg, float *xy)
+{
+    std::vector<float> s(nx);
+    float step = (float)(1.0 / nx);
+    s[0] = (float)(-1.0 / 2);
+    for (int k = 1; k < nx; ++k) s[k] = s[k - 1] + step;
+    for (int i = 0; i < nz; ++i) {
+        double a = (double)th_neg[i] * kRefPiPx2d / 180;
+        double c = std::cos(a), sn = std::sin(a);
+        for (int k = 0; k < nx; ++k) {
+            xy[2 * ((size_t)i * nx + k)] = (float)((double)s[k] * c);
+            xy[2 * ((size_t)i * nx + k) + 1] = (float)((double)s[k] * sn);
+        }
+    }
+}
+
+// weight.cu:8-41.
+void weights(int nx, int nz, const float *t, float *w)
+{
+    int center = nx / 2;
+    for (int i = 0; i < nz; ++i)
+        for (int j = 0; j < nx; ++j) {
+            float v;
+            if (j == center) v = (float)(180.0 / (4 * nz));
+            else if (i == 0) v = (float)(2.0 * std::fabs((t[i + 1] - t[i]) * (float)(j - center)));
+            else if (i == nz - 1) v = (float)(2.0 * std::fabs((t[i - 1] - t[i]) * (float)(j - center)));
+            else v = (float)(1.0 * std::fabs((t[i - 1] - t[i + 1]) * (float)(j - center)));
+            w[(size_t)i * nx + j] = v;
+        }
+}
+
+// Deapodisation factors (NU:22-42): exp(-b (pi k/n)^2) in double, stored as float.
+std::vector<float> deapod(int N, int n, float b)
+{
+    std::vector<float> c(N);
+    for (int X = 0; X < N; ++X) {
+        int k = X - N / 2;
+        c[X] = (float)std::exp(-(double)b * ((kRefPi * k / (double)n) * (kRefPi * k / (double)n)));
+    }
+    return c;
+}
+
+std::vector<float2> twiddles(int n)
+{
+    std::vector<float2> t(n);
+    for (int q = 0; q < n; ++q) {
+        double a = 2.0 * M_PI * (double)q / (double)n;
+        t[q] = make_float2((float)std::cos(a), (float)-std::sin(a));
+    }
+    return t;
+}
+
+int ilog2(int n)
+{
+    int l = 0;
+    while ((1 << l) < n) ++l;
+    return l;
+}
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+};
+
+// Owned device allocations of a plan.
+struct Arena {
+    std::vector<std::unique_ptr<DevBuf>> bufs;
+    size_t total = 0;
+    template <typename T>
+    icon_status alloc(T **out, size_t count)
+    {
+        auto b = std::make_unique<DevBuf>();
+        size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+        cudaError_t e = cudaMalloc(&b->p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ICON_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+        }
+        b->bytes = bytes;
+        total += bytes;
+        *out = (T *)b->p;
+        bufs.push_back(std::move(b));
+        return ICON_OK;
+    }
+    template <typename T>
+    icon_status upload(T **out, const T *host, size_t count)
+    {
+        ICON_TRY(alloc(out, count));
+        ICON_CUDA(cudaMemcpy(*out, host, count * sizeof(T), cudaMemcpyHostToDevice));
+        return ICON_OK;
+    }
+};
+
+// Node tables of one geometry (a tilt series or a single reprojection line).
+struct NodeTables {
+    int M = 0;
+    float *phix = nullptr, *phiy = nullptr, *w = nullptr;
+    int *ix0 = nullptr, *iy0 = nullptr, *row_off = nullptr, *ent_jt = nullptr, *ent_iy0 = nullptr;
+};
+
+}  // namespace
+
+struct icon_plan {
+    int dev = 0;
+    int nx = 0, N0 = 0, N1 = 0, nz = 0, M = 0, n0 = 0, n1 = 0, lg0 = 0, lg1 = 0;
+    int B = 1, cap = 0, Gcap = 0;
+    float th0 = 0, th1 = 0, b0 = 0, bf0 = 0, b1 = 0, bf1 = 0;
+    std::vector<float> tlt, th_neg, xy, w;
+    int omit_index = 0;
+    Arena arena;
+    NodeTables nodes;
+    float *cx = nullptr, *cy = nullptr, *phi1 = nullptr;
+    int *i10 = nullptr;
+    float2 *tw0 = nullptr, *tw1 = nullptr;
+    // scratch sized for Gcap groups
+    float2 *G1 = nullptr, *P = nullptr, *f = nullptr, *rhat = nullptr, *Ahwb = nullptr, *imgc = nullptr;
+    float *m = nullptr, *rows = nullptr, *outrp = nullptr, *mout = nullptr;
+    double *part_rtr = nullptr, *part_rtar = nullptr, *alpha = nullptr;
+    int k3_blocks = 0;
+    // reprojection lines, keyed by the .tlt angle
+    std::map<float, std::unique_ptr<NodeTables>> lines;
+    float2 *fline = nullptr;
+    size_t smem_x = 0, smem_y = 0;
+    int thr_x = 0, thr_y = 0;
+    // tracing: events around every launch while enabled
+    bool trace = false;
+    long long launches = 0;
+    struct Pending {
+        int kind;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t ev_get()
+    {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    ~icon_plan()
+    {
+        for (auto &q : pending) {
+            cudaEventDestroy(q.a);
+            cudaEventDestroy(q.b);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+
+    Geo geo(const NodeTables &t) const
+    {
+        Geo g;
+        g.N0 = N0; g.N1 = N1; g.n0 = n0; g.n1 = n1; g.lg0 = lg0; g.lg1 = lg1;
+        g.M = t.M; g.nx = nx; g.nz = nz; g.B = B;
+        g.w = t.w; g.phix = t.phix; g.phiy = t.phiy; g.ix0 = t.ix0; g.iy0 = t.iy0;
+        g.cx = cx; g.cy = cy; g.row_off = t.row_off; g.ent_jt = t.ent_jt; g.ent_iy0 = t.ent_iy0;
+        g.tw0 = tw0; g.tw1 = tw1;
+        return g;
+    }
+    Geo1 geo1() const
+    {
+        Geo1 g;
+        g.phi1 = phi1;
+        g.i10 = i10;
+        return g;
+    }
+};
+
+namespace {
+
+enum Kind { K_XF = 0, K_YF, K_FIN, K_YA, K_XA, K_ALPHA, K_UPD, K_ROWS, K_LAYOUT, K_ROWADJ };
+
+// Launches one kernel; counts it and, while tracing, brackets it by events
+// and records its algorithmic bytes (compulsory reads + writes, see
+// algo_bytes below).
+#define LAUNCH_B(p, kind, st, bytes, ...)                                 \
+    do {                                                                  \
+        cudaEvent_t e0_ = nullptr;                                        \
+        if ((p)->trace) {                                                 \
+            e0_ = (p)->ev_get();                                          \
+            cudaEventRecord(e0_, st);                                     \
+        }                                                                 \
+        __VA_ARGS__;                                                      \
+        (p)->launches++;                                                  \
+        if ((p)->trace) {                                                 \
+            cudaEvent_t e1_ = (p)->ev_get();                              \
+            cudaEventRecord(e1_, st);                                     \
+            (p)->pending.push_back({kind, e0_, e1_, (double)(bytes)});    \
+        }                                                                 \
+    } while (0)
+#define LAUNCH(p, kind, st, ...) LAUNCH_B(p, kind, st, 0.0, __VA_ARGS__)
+
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// Builds window tables and the per-row entry lists of M nodes at xy.
+icon_status build_tables(icon_plan *p, const float *xy, const float *w, int M, NodeTables &t)
+{
+    t.M = M;
+    float *xy_d = nullptr;
+    ICON_TRY(p->arena.upload(&xy_d, xy, (size_t)2 * M));
+    ICON_TRY(p->arena.alloc(&t.phix, (size_t)M * kTaps));
+    ICON_TRY(p->arena.alloc(&t.phiy, (size_t)M * kTaps));
+    ICON_TRY(p->arena.alloc(&t.ix0, (size_t)M));
+    ICON_TRY(p->arena.alloc(&t.iy0, (size_t)M));
+    int blk = 256, grd = (M + blk - 1) / blk;
+    icon::k_window<<<grd, blk>>>(xy_d, 2, M, p->n0, p->b0, p->bf0, t.phix, t.ix0);
+    icon::k_window<<<grd, blk>>>(xy_d + 1, 2, M, p->n1, p->b1, p->bf1, t.phiy, t.iy0);
+    ICON_CUDA(cudaGetLastError());
+    std::vector<int> ix0(M), iy0(M);
+    ICON_CUDA(cudaMemcpy(ix0.data(), t.ix0, sizeof(int) * M, cudaMemcpyDeviceToHost));
+    ICON_CUDA(cudaMemcpy(iy0.data(), t.iy0, sizeof(int) * M, cudaMemcpyDeviceToHost));
+    // Entries (node j, x tap t0) grouped by grid row x = (ix0 + t0) mod n0,
+    // sorted within a row by (iy0, j).
+    const int n0 = p->n0;
+    std::vector<int> cnt(n0 + 1, 0);
+    for (int j = 0; j < M; ++j)
+        for (int t0 = 0; t0 < kTaps; ++t0) cnt[((ix0[j] + t0) % n0 + n0) % n0 + 1]++;
+    for (int x = 0; x < n0; ++x) cnt[x + 1] += cnt[x];
+    std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+    size_t E = (size_t)M * kTaps;
+    std::vector<int> jt(E), ky(E);
+    for (int j = 0; j < M; ++j)
+        for (int t0 = 0; t0 < kTaps; ++t0) {
+            int x = ((ix0[j] + t0) % n0 + n0) % n0;
+            int e = pos[x]++;
+            jt[e] = j * 16 + t0;
+            ky[e] = iy0[j];
+        }
+    std::vector<int> order;
+    std::vector<int> jt2(E), ky2(E);
+    for (int x = 0; x < n0; ++x) {
+        int a = cnt[x], c = cnt[x + 1];
+        order.resize(c - a);
+        for (int i = 0; i < c - a; ++i) order[i] = a + i;
+        std::stable_sort(order.begin(), order.end(), [&](int u, int v) {
+            return ky[u] != ky[v] ? ky[u] < ky[v] : jt[u] < jt[v];
+        });
+        for (int i = 0; i < c - a; ++i) {
+            jt2[a + i] = jt[order[i]];
+            ky2[a + i] = ky[order[i]];
+        }
+    }
+    ICON_TRY(p->arena.upload(&t.row_off, cnt.data(), (size_t)n0 + 1));
+    ICON_TRY(p->arena.upload(&t.ent_jt, jt2.data(), E));
+    ICON_TRY(p->arena.upload(&t.ent_iy0, ky2.data(), E));
+    ICON_TRY(p->arena.upload(&t.w, w, (size_t)M));
+    return ICON_OK;
+}
+
+icon_status check_plan(const icon_plan *p, int S)
+{
+    if (!p) return fail(ICON_ERR_INVALID, "null plan");
+    if (S < 1) return fail(ICON_ERR_INVALID, "S must be >= 1");
+    if (S > p->cap) return fail(ICON_ERR_CAPACITY, "S = " + std::to_string(S) + " exceeds plan capacity " + std::to_string(p->cap));
+    return ICON_OK;
+}
+
+inline int groups(const icon_plan *p, int S) { return (S + p->B - 1) / p->B; }
+
+inline int grid1d(size_t total)
+{
+    size_t b = (total + 255) / 256;
+    return (int)std::min<size_t>(std::max<size_t>(b, 1), 148 * 16);
+}
+
+// ------------------------------------------------------------- stages ----
+// Algorithmic bytes per slot (one slice of a group) of each stage: the data a
+// stage must read and write at least once; per-group tables are divided by B.
+struct StageBytes {
+    double xf_real, xf_cplx, yf, fin_store, fin_red, ya, xa_plain, xa_resid, upd;
+};
+StageBytes stage_bytes(const icon_plan *p, const NodeTables &t)
+{
+    StageBytes b;
+    double NN = (double)p->N0 * p->N1, G1 = (double)p->n0 * p->N1 * 8, MT = (double)t.M * kTaps, B = p->B;
+    b.xf_real = NN * 4 + G1;
+    b.xf_cplx = NN * 8 + G1;
+    b.yf = G1 + MT * 8 + (MT * 8 + MT * 4) / B;            // G1 row reads, P writes; entries + phiy
+    b.fin_store = MT * 8 + (double)t.M * 8 + (MT * 4 + t.M * 4) / B;
+    b.fin_red = MT * 8 + (MT * 4 + t.M * 4) / B;
+    b.ya = (double)t.M * 8 + G1 + (MT * 8 + MT * 8) / B;   // f, G1 writes; entries + phix/phiy
+    b.xa_plain = G1 + NN * 8;
+    b.xa_resid = G1 + NN * 16;
+    b.upd = NN * 16;
+    return b;
+}
+
+icon_status launch_forward(icon_plan *p, const NodeTables &t, const void *img_int, bool real_in, int G, int mode,
+                           float2 *f_out, cudaStream_t st)
+{
+    Geo g = p->geo(t);
+    const StageBytes sb = stage_bytes(p, t);
+    const double slots = (double)G * p->B;
+    dim3 gx(p->N1, G), gy(p->n0, G);
+    if (real_in) LAUNCH_B(p, K_XF, st, sb.xf_real * slots, icon::k_xpass_fwd<true><<<gx, p->thr_x, p->smem_x, st>>>(g, img_int, p->G1));
+    else LAUNCH_B(p, K_XF, st, sb.xf_cplx * slots, icon::k_xpass_fwd<false><<<gx, p->thr_x, p->smem_x, st>>>(g, img_int, p->G1));
+    LAUNCH_B(p, K_YF, st, sb.yf * slots, icon::k_ypass_fwd<<<gy, p->thr_y, p->smem_y, st>>>(g, p->G1, p->P));
+    int kb = (t.M * p->B + 255) / 256;
+    dim3 g3(kb, G);
+    if (mode == 0) LAUNCH_B(p, K_FIN, st, sb.fin_store * slots, icon::k_interp_fin<0><<<g3, 256, 0, st>>>(g, p->P, f_out, nullptr));
+    else if (mode == 1) LAUNCH_B(p, K_FIN, st, sb.fin_store * slots, icon::k_interp_fin<1><<<g3, 256, 0, st>>>(g, p->P, f_out, nullptr));
+    else LAUNCH_B(p, K_FIN, st, sb.fin_red * slots, icon::k_interp_fin<2><<<g3, 256, 0, st>>>(g, p->P, nullptr, p->part_rtar));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+icon_status launch_adjoint(icon_plan *p, const float2 *f_int, int G, int mode, float2 *out_int, cudaStream_t st)
+{
+    Geo g = p->geo(p->nodes);
+    const StageBytes sb = stage_bytes(p, p->nodes);
+    const double slots = (double)G * p->B;
+    dim3 gy(p->n0, G), gx(p->N1, G);
+    LAUNCH_B(p, K_YA, st, sb.ya * slots, icon::k_ypass_adj<<<gy, p->thr_y, p->smem_y, st>>>(g, f_int, p->G1));
+    size_t smem = p->smem_x + sizeof(double) * p->thr_x;
+    if (mode == 0) LAUNCH_B(p, K_XA, st, sb.xa_plain * slots, icon::k_xpass_adj<0><<<gx, p->thr_x, smem, st>>>(g, p->G1, out_int, nullptr, nullptr));
+    else LAUNCH_B(p, K_XA, st, sb.xa_resid * slots, icon::k_xpass_adj<1><<<gx, p->thr_x, smem, st>>>(g, p->G1, out_int, p->Ahwb, p->part_rtr));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+icon_status launch_rows(icon_plan *p, const float *d_rows, int S, int G, float2 *bout, cudaStream_t st)
+{
+    Geo g = p->geo(p->nodes);
+    LAUNCH(p, K_ROWS, st, icon::k_rows_fwd<<<dim3(p->nz, G), p->thr_x, p->smem_x, st>>>(g, p->geo1(), d_rows, S, p->f, bout));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+// One ICON iteration over G groups (Iteration2.cu:53-132 with Alpha2).
+icon_status launch_iteration(icon_plan *p, int G, bool clamp, int data_type, float thr, double *hist_a, double *hist_r,
+                             cudaStream_t st)
+{
+    ICON_TRY(launch_forward(p, p->nodes, p->m, true, G, 1, p->f, st));          // f = W A m
+    ICON_TRY(launch_adjoint(p, p->f, G, 1, p->rhat, st));                       // rhat = A^H f - Ahwb, ||rhat||^2
+    ICON_TRY(launch_forward(p, p->nodes, p->rhat, false, G, 2, nullptr, st));   // r = A rhat, sum w|r|^2
+    int kb = (p->M * p->B + 255) / 256;
+    LAUNCH(p, K_ALPHA, st, icon::k_alpha<<<G, 32 * p->B, 0, st>>>(p->part_rtr, p->N1, p->part_rtar, kb, p->B, p->alpha, hist_a, hist_r));
+    size_t per_group = (size_t)p->N1 * p->N0 * p->B, total = per_group * G;
+    LAUNCH_B(p, K_UPD, st, stage_bytes(p, p->nodes).upd * G * p->B, icon::k_update<<<grid1d(total), 256, 0, st>>>(p->m, p->rhat, p->alpha, p->B, per_group, total,
+                                                                       clamp ? 1 : 0, data_type, thr));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+icon_status line_tables(icon_plan *p, float tilt_deg, NodeTables **out)
+{
+    auto it = p->lines.find(tilt_deg);
+    if (it != p->lines.end()) {
+        *out = it->second.get();
+        return ICON_OK;
+    }
+    auto t = std::make_unique<NodeTables>();
+    float thn = -tilt_deg;
+    std::vector<float> xy((size_t)2 * p->nx), w((size_t)p->nx, 1.0f);
+    px2d(p->nx, 1, &thn, xy.data());
+    ICON_TRY(build_tables(p, xy.data(), w.data(), p->nx, *t));
+    *out = t.get();
+    p->lines[tilt_deg] = std::move(t);
+    return ICON_OK;
+}
+
+icon_status reproject_internal(icon_plan *p, const float *m_int, float tilt_deg, float *d_out, int S, cudaStream_t st)
+{
+    NodeTables *lt = nullptr;
+    ICON_TRY(line_tables(p, tilt_deg, &lt));
+    int G = groups(p, S);
+    ICON_TRY(launch_forward(p, *lt, m_int, true, G, 0, p->fline, st));
+    Geo g = p->geo(*lt);
+    LAUNCH(p, K_ROWADJ, st, icon::k_row_adj<<<G, p->thr_x, p->smem_x, st>>>(g, p->geo1(), p->fline, d_out, S));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+}  // namespace
+
+// ================================================================ C ABI ====
+extern "C" {
+
+const char *icon_last_error(void) { return g_last_error.c_str(); }
+
+icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
+{
+    if (!geo || !out) return fail(ICON_ERR_INVALID, "null argument");
+    *out = nullptr;
+    int nx = geo->nx, N1 = geo->thickness == 0 ? geo->nx : geo->thickness, nz = geo->ntilt;
+    if (nx < 8 || N1 < 8) return fail(ICON_ERR_INVALID, "nx and thickness must be >= 8");
+    if (nx > 4096 || N1 > 4096) return fail(ICON_ERR_INVALID, "nx and thickness must be <= 4096");
+    if (nz < 2 || !geo->tilt_deg) return fail(ICON_ERR_INVALID, "need at least 2 tilt angles");
+    if (geo->capacity < 1) return fail(ICON_ERR_INVALID, "capacity must be >= 1");
+    if ((long long)nx * nz * kTaps >= (1LL << 27)) return fail(ICON_ERR_INVALID, "too many nodes");
+    int dev = geo->device;
+    if (dev < 0) {
+        if (cudaGetDevice(&dev) != cudaSuccess) return fail(ICON_ERR_CUDA, "no CUDA device");
+    }
+    DeviceGuard guard(dev);
+    if (!guard.ok) return fail(ICON_ERR_CUDA, "cudaSetDevice failed");
+    auto p = std::make_unique<icon_plan>();
+    p->dev = dev;
+    p->nx = nx;
+    p->N0 = nx;
+    p->N1 = N1;
+    p->nz = nz;
+    p->M = nx * nz;
+    grid_params(p->N0, p->th0, p->n0, p->b0, p->bf0);
+    grid_params(p->N1, p->th1, p->n1, p->b1, p->bf1);
+    p->lg0 = ilog2(p->n0);
+    p->lg1 = ilog2(p->n1);
+    int nmax = std::max(p->n0, p->n1);
+    int B = nmax <= 2048 ? 8 : (nmax <= 4096 ? 4 : 2);
+    while (B > 1 && B / 2 >= geo->capacity) B /= 2;
+    p->B = B;
+    p->cap = geo->capacity;
+    p->Gcap = (geo->capacity + B - 1) / B;
+    p->tlt.assign(geo->tilt_deg, geo->tilt_deg + nz);
+    p->th_neg.resize(nz);
+    for (int i = 0; i < nz; ++i) p->th_neg[i] = -p->tlt[i];   // MainCode.cu:42
+    float om = p->th_neg[0];
+    p->omit_index = 0;
+    for (int i = 0; i < nz; ++i)                                // MainCode.cu:46-49
+        if (std::fabs(om) > std::fabs(p->th_neg[i])) {
+            om = p->th_neg[i];
+            p->omit_index = i;
+        }
+    p->xy.resize((size_t)2 * p->M);
+    p->w.resize(p->M);
+    px2d(nx, nz, p->th_neg.data(), p->xy.data());
+    weights(nx, nz, p->th_neg.data(), p->w.data());
+    ICON_TRY(build_tables(p.get(), p->xy.data(), p->w.data(), p->M, p->nodes));
+    std::vector<float> cx = deapod(p->N0, p->n0, p->b0), cy = deapod(p->N1, p->n1, p->b1);
+    ICON_TRY(p->arena.upload(&p->cx, cx.data(), cx.size()));
+    ICON_TRY(p->arena.upload(&p->cy, cy.data(), cy.size()));
+    // 1-D row transform nodes (k - nx/2)/nx (MainCode.cu:72-80).
+    std::vector<float> px1((size_t)nx);
+    for (int k = 0; k < nx; ++k) px1[k] = (float)(((double)(float)k - (double)(float)nx / 2.0) / (double)(float)nx);
+    float *px1_d = nullptr;
+    ICON_TRY(p->arena.upload(&px1_d, px1.data(), px1.size()));
+    ICON_TRY(p->arena.alloc(&p->phi1, (size_t)nx * kTaps));
+    ICON_TRY(p->arena.alloc(&p->i10, (size_t)nx));
+    icon::k_window<<<(nx + 255) / 256, 256>>>(px1_d, 1, nx, p->n0, p->b0, p->bf0, p->phi1, p->i10);
+    ICON_CUDA(cudaGetLastError());
+    std::vector<float2> t0 = twiddles(p->n0), t1 = twiddles(p->n1);
+    ICON_TRY(p->arena.upload(&p->tw0, t0.data(), t0.size()));
+    ICON_TRY(p->arena.upload(&p->tw1, t1.data(), t1.size()));
+    // Launch shapes: one thread per 16 values of an [n][B] FFT buffer.
+    p->thr_x = p->n0 * B / 16;
+    p->thr_y = p->n1 * B / 16;
+    p->smem_x = (size_t)p->n0 * B * sizeof(float2);
+    p->smem_y = (size_t)p->n1 * B * sizeof(float2);
+    int smem_max = 0;
+    ICON_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    size_t need_x = p->smem_x + sizeof(double) * p->thr_x;
+    if ((size_t)smem_max < std::max(need_x, p->smem_y)) return fail(ICON_ERR_INVALID, "FFT buffer exceeds shared memory");
+    ICON_CUDA(cudaFuncSetAttribute(icon::k_xpass_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_x));
+    ICON_CUDA(cudaFuncSetAttribute(icon::k_xpass_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_x));
+    ICON_CUDA(cudaFuncSetAttribute(icon::k_ypass_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_y));
+    ICON_CUDA(cudaFuncSetAttribute(icon::k_ypass_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_y));
+    ICON_CUDA(cudaFuncSetAttribute(icon::k_xpass_adj<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_x));
+    ICON_CUDA(cudaFuncSetAttribute(icon::k_xpass_adj<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_x));
+    ICON_CUDA(cudaFuncSetAttribute(icon::k_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_x));
+    ICON_CUDA(cudaFuncSetAttribute(icon::k_row_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_x));
+    // Scratch for Gcap groups.
+    size_t G = p->Gcap, Bz = B;
+    ICON_TRY(p->arena.alloc(&p->G1, G * p->n0 * p->N1 * Bz));
+    ICON_TRY(p->arena.alloc(&p->P, G * p->M * kTaps * Bz));
+    ICON_TRY(p->arena.alloc(&p->f, G * p->M * Bz));
+    ICON_TRY(p->arena.alloc(&p->fline, G * p->nx * Bz));
+    size_t NN = (size_t)p->N0 * p->N1;
+    ICON_TRY(p->arena.alloc(&p->rhat, G * NN * Bz));
+    ICON_TRY(p->arena.alloc(&p->Ahwb, G * NN * Bz));
+    ICON_TRY(p->arena.alloc(&p->imgc, G * NN * Bz));
+    ICON_TRY(p->arena.alloc(&p->m, G * NN * Bz));
+    ICON_TRY(p->arena.alloc(&p->rows, (size_t)p->cap * nz * nx));
+    ICON_TRY(p->arena.alloc(&p->outrp, (size_t)p->cap * nx));
+    ICON_TRY(p->arena.alloc(&p->mout, (size_t)p->cap * NN));
+    p->k3_blocks = (p->M * B + 255) / 256;
+    ICON_TRY(p->arena.alloc(&p->part_rtr, G * p->N1 * Bz));
+    ICON_TRY(p->arena.alloc(&p->part_rtar, G * p->k3_blocks * Bz));
+    ICON_TRY(p->arena.alloc(&p->alpha, G * Bz));
+    ICON_CUDA(cudaDeviceSynchronize());
+    *out = p.release();
+    return ICON_OK;
+}
+
+icon_status icon_plan_destroy(icon_plan *plan)
+{
+    if (!plan) return ICON_OK;
+    DeviceGuard guard(plan->dev);
+    cudaDeviceSynchronize();
+    delete plan;
+    return ICON_OK;
+}
+
+icon_status icon_plan_query(const icon_plan *p, int *dims)
+{
+    if (!p || !dims) return fail(ICON_ERR_INVALID, "null argument");
+    dims[0] = p->N0; dims[1] = p->N1; dims[2] = p->n0; dims[3] = p->n1; dims[4] = p->M;
+    dims[5] = p->nz; dims[6] = p->B; dims[7] = p->cap;
+    dims[8] = (int)std::min<size_t>(p->arena.total >> 20, 0x7fffffff);
+    dims[9] = p->omit_index;
+    return ICON_OK;
+}
+
+icon_status icon_plan_geometry(const icon_plan *p, float *h_xy, float *h_w)
+{
+    if (!p) return fail(ICON_ERR_INVALID, "null plan");
+    if (h_xy) std::memcpy(h_xy, p->xy.data(), sizeof(float) * p->xy.size());
+    if (h_w) std::memcpy(h_w, p->w.data(), sizeof(float) * p->w.size());
+    return ICON_OK;
+}
+
+icon_status icon_nufft_forward(icon_plan *p, const float *d_img, void *d_nodes, int S, void *stream)
+{
+    ICON_TRY(check_plan(p, S));
+    if (!d_img || !d_nodes) return fail(ICON_ERR_INVALID, "null buffer");
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    int G = groups(p, S);
+    size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
+    LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float><<<grid1d(tot), 256, 0, st>>>(d_img, p->m, S, p->N0, p->N1, p->B, tot));
+    ICON_TRY(launch_forward(p, p->nodes, p->m, true, G, 0, p->f, st));
+    LAUNCH(p, K_LAYOUT, st, icon::k_nodes_out<<<grid1d((size_t)S * p->M), 256, 0, st>>>(p->f, (float2 *)d_nodes, S, p->M, p->B));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+icon_status icon_nufft_forward_complex(icon_plan *p, const void *d_img, void *d_nodes, int S, void *stream)
+{
+    ICON_TRY(check_plan(p, S));
+    if (!d_img || !d_nodes) return fail(ICON_ERR_INVALID, "null buffer");
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    int G = groups(p, S);
+    size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
+    LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float2><<<grid1d(tot), 256, 0, st>>>((const float2 *)d_img, p->imgc, S, p->N0, p->N1, p->B, tot));
+    ICON_TRY(launch_forward(p, p->nodes, p->imgc, false, G, 0, p->f, st));
+    LAUNCH(p, K_LAYOUT, st, icon::k_nodes_out<<<grid1d((size_t)S * p->M), 256, 0, st>>>(p->f, (float2 *)d_nodes, S, p->M, p->B));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+icon_status icon_nufft_adjoint(icon_plan *p, const void *d_nodes, void *d_img, int S, void *stream)
+{
+    ICON_TRY(check_plan(p, S));
+    if (!d_img || !d_nodes) return fail(ICON_ERR_INVALID, "null buffer");
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    int G = groups(p, S);
+    size_t tot = (size_t)G * p->M * p->B;
+    LAUNCH(p, K_LAYOUT, st, icon::k_nodes_in<<<grid1d(tot), 256, 0, st>>>((const float2 *)d_nodes, p->f, S, p->M, p->B, tot));
+    ICON_TRY(launch_adjoint(p, p->f, G, 0, p->imgc, st));
+    LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float2><<<grid1d((size_t)S * p->N0 * p->N1), 256, 0, st>>>(p->imgc, (float2 *)d_img, S, p->N0, p->N1, p->B));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+icon_status icon_rows_forward(icon_plan *p, const float *d_rows, void *d_b, int S, void *stream)
+{
+    ICON_TRY(check_plan(p, S));
+    if (!d_rows || !d_b) return fail(ICON_ERR_INVALID, "null buffer");
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    int G = groups(p, S);
+    ICON_TRY(launch_rows(p, d_rows, S, G, p->P, st));   // unweighted b into scratch
+    LAUNCH(p, K_LAYOUT, st, icon::k_nodes_out<<<grid1d((size_t)S * p->M), 256, 0, st>>>(p->P, (float2 *)d_b, S, p->M, p->B));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+icon_status icon_prepare_rhs(icon_plan *p, const float *d_rows, void *d_Ahwb, int S, void *stream)
+{
+    ICON_TRY(check_plan(p, S));
+    if (!d_rows || !d_Ahwb) return fail(ICON_ERR_INVALID, "null buffer");
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    int G = groups(p, S);
+    ICON_TRY(launch_rows(p, d_rows, S, G, nullptr, st));
+    ICON_TRY(launch_adjoint(p, p->f, G, 0, p->imgc, st));
+    LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float2><<<grid1d((size_t)S * p->N0 * p->N1), 256, 0, st>>>(p->imgc, (float2 *)d_Ahwb, S, p->N0, p->N1, p->B));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+icon_status icon_solve(icon_plan *p, const icon_solve_cfg *cfg, const void *d_Ahwb, float *d_m, int S, int warm_start,
+                       double *h_alpha, double *h_rtr, void *stream)
+{
+    ICON_TRY(check_plan(p, S));
+    if (!cfg || !d_Ahwb || !d_m) return fail(ICON_ERR_INVALID, "null argument");
+    int a = cfg->infr_before, b = cfg->icon, c = cfg->infr_after;
+    if (a < 0 || b < 0 || c < 0) return fail(ICON_ERR_INVALID, "negative iteration count");
+    int iters = a + b + c;
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    int G = groups(p, S);
+    size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
+    LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float2><<<grid1d(tot), 256, 0, st>>>((const float2 *)d_Ahwb, p->Ahwb, S, p->N0, p->N1, p->B, tot));
+    if (warm_start) LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float><<<grid1d(tot), 256, 0, st>>>(d_m, p->m, S, p->N0, p->N1, p->B, tot));
+    else ICON_CUDA(cudaMemsetAsync(p->m, 0, tot * sizeof(float), st));
+    double *hist = nullptr;
+    size_t slots = (size_t)G * p->B;
+    bool want_hist = (h_alpha || h_rtr) && iters > 0;
+    if (want_hist) ICON_CUDA(cudaMalloc(&hist, sizeof(double) * 2 * slots * iters));
+    icon_status rc = ICON_OK;
+    for (int it = 0; it < iters && rc == ICON_OK; ++it) {
+        bool clamp = (a <= it && it < iters - c);              // Iteration2.cu:129
+        double *ha = want_hist ? hist + (size_t)it * slots : nullptr;
+        double *hr = want_hist ? hist + (size_t)(iters + it) * slots : nullptr;
+        rc = launch_iteration(p, G, clamp, cfg->data_type, cfg->threshold, ha, hr, st);
+    }
+    if (rc == ICON_OK) {
+        LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float><<<grid1d((size_t)S * p->N0 * p->N1), 256, 0, st>>>(p->m, d_m, S, p->N0, p->N1, p->B));
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (want_hist) {
+        std::vector<double> hv(2 * slots * iters);
+        cudaError_t e = cudaMemcpyAsync(hv.data(), hist, sizeof(double) * hv.size(), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        cudaFree(hist);
+        if (e != cudaSuccess && rc == ICON_OK) rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+        if (rc == ICON_OK)
+            for (int it = 0; it < iters; ++it)
+                for (int s = 0; s < S; ++s) {
+                    if (h_alpha) h_alpha[(size_t)it * S + s] = hv[(size_t)it * slots + s];
+                    if (h_rtr) h_rtr[(size_t)it * S + s] = hv[(size_t)(iters + it) * slots + s];
+                }
+    }
+    return rc;
+}
+
+icon_status icon_reproject(icon_plan *p, const float *d_m, float tilt_deg, float *d_out, int S, void *stream)
+{
+    ICON_TRY(check_plan(p, S));
+    if (!d_m || !d_out) return fail(ICON_ERR_INVALID, "null buffer");
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    int G = groups(p, S);
+    size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
+    LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float><<<grid1d(tot), 256, 0, st>>>(d_m, p->m, S, p->N0, p->N1, p->B, tot));
+    ICON_CUDA(cudaGetLastError());
+    return reproject_internal(p, p->m, tilt_deg, d_out, S, st);
+}
+
+icon_status icon_reconstruct_host(icon_plan *p, const icon_solve_cfg *cfg, const float *h_rows, float *h_m,
+                                  float *h_reproj, int S, void *stream)
+{
+    if (!p || !cfg || !h_rows || !h_m) return fail(ICON_ERR_INVALID, "null argument");
+    if (S < 1) return fail(ICON_ERR_INVALID, "S must be >= 1");
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    bool own = (st == nullptr);
+    if (own) ICON_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    icon_status rc = ICON_OK;
+    size_t R = (size_t)p->nz * p->nx, NN = (size_t)p->N0 * p->N1;
+    float *d_mo = p->mout;
+    int a = cfg->infr_before, b = cfg->icon, c = cfg->infr_after, iters = a + b + c;
+    for (int s0 = 0; s0 < S && rc == ICON_OK; s0 += p->cap) {
+        int Sc = std::min(p->cap, S - s0);
+        int G = groups(p, Sc);
+        cudaError_t e = cudaMemcpyAsync(p->rows, h_rows + (size_t)s0 * R, sizeof(float) * R * Sc, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) { rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e)); break; }
+        if ((rc = launch_rows(p, p->rows, Sc, G, nullptr, st)) != ICON_OK) break;
+        if ((rc = launch_adjoint(p, p->f, G, 0, p->Ahwb, st)) != ICON_OK) break;
+        size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
+        if ((e = cudaMemsetAsync(p->m, 0, tot * sizeof(float), st)) != cudaSuccess) { rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e)); break; }
+        for (int it = 0; it < iters && rc == ICON_OK; ++it)
+            rc = launch_iteration(p, G, a <= it && it < iters - c, cfg->data_type, cfg->threshold, nullptr, nullptr, st);
+        if (rc != ICON_OK) break;
+        LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float><<<grid1d((size_t)Sc * NN), 256, 0, st>>>(p->m, d_mo, Sc, p->N0, p->N1, p->B));
+        if (h_reproj && (rc = reproject_internal(p, p->m, p->tlt[p->omit_index], p->outrp, Sc, st)) != ICON_OK) break;
+        if ((e = cudaMemcpyAsync(h_m + (size_t)s0 * NN, d_mo, sizeof(float) * NN * Sc, cudaMemcpyDeviceToHost, st)) != cudaSuccess) {
+            rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+            break;
+        }
+        if (h_reproj && (e = cudaMemcpyAsync(h_reproj + (size_t)s0 * p->nx, p->outrp, sizeof(float) * p->nx * Sc,
+                                             cudaMemcpyDeviceToHost, st)) != cudaSuccess) {
+            rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+            break;
+        }
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaStreamSynchronize(st);
+    if (own) cudaStreamDestroy(st);
+    return rc;
+}
+
+icon_status icon_trace_enable(icon_plan *p, int enable)
+{
+    if (!p) return fail(ICON_ERR_INVALID, "null plan");
+    p->trace = enable != 0;
+    return ICON_OK;
+}
+
+icon_status icon_trace_read(icon_plan *p, int *h_count, double *h_ms, double *h_bytes)
+{
+    if (!p || !h_count || !h_ms) return fail(ICON_ERR_INVALID, "null argument");
+    DeviceGuard guard(p->dev);
+    for (int k = 0; k < ICON_TRACE_KERNELS; ++k) {
+        h_count[k] = 0;
+        h_ms[k] = 0.0;
+        if (h_bytes) h_bytes[k] = 0.0;
+    }
+    icon_status rc = ICON_OK;
+    for (auto &q : p->pending) {
+        float ms = 0.f;
+        cudaError_t e = cudaEventSynchronize(q.b);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, q.a, q.b);
+        if (e != cudaSuccess && rc == ICON_OK) rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+        if (q.kind >= 0 && q.kind < ICON_TRACE_KERNELS) {
+            h_count[q.kind]++;
+            h_ms[q.kind] += ms;
+            if (h_bytes) h_bytes[q.kind] += q.bytes;
+        }
+        p->pool.push_back(q.a);
+        p->pool.push_back(q.b);
+    }
+    p->pending.clear();
+    return rc;
+}
+
+long long icon_launch_count(const icon_plan *p) { return p ? p->launches : 0; }
+
+}  // extern "C"

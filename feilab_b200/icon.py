@@ -1,0 +1,236 @@
+"""Python binding of the C ABI in include/icon_b200.h (ctypes, torch tensors).
+
+This mirrors the reference's per-slice routines of ICON-GPU v1.2.9
+(nufft_gpu_v8.cu: cunfft_trafo_2d_R2C2, cunfft_trafo_2d2, cunfft_adjoint_2d2;
+readSlicePart; Iteration3; reProject_NFFT2) as batched calls on a plan.  All
+device arrays are torch CUDA tensors on the plan's device; work is queued on
+torch's current stream.  Errors raise IconError with the library's message.
+
+The library must have been built (python -m feilab_b200.build); there is no
+fallback: importing on a machine without it raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libicon_b200.so")
+
+_lib = None
+
+
+class IconError(RuntimeError):
+    pass
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise IconError(f"native library {LIB_PATH} is missing; build it with `python -m feilab_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, F, V = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_void_p
+        L.icon_plan_create.argtypes = [ctypes.POINTER(Geometry), ctypes.POINTER(P)]
+        L.icon_plan_destroy.argtypes = [P]
+        L.icon_plan_query.argtypes = [P, ctypes.POINTER(I)]
+        L.icon_plan_geometry.argtypes = [P, V, V]
+        L.icon_nufft_forward.argtypes = [P, V, V, I, V]
+        L.icon_nufft_forward_complex.argtypes = [P, V, V, I, V]
+        L.icon_nufft_adjoint.argtypes = [P, V, V, I, V]
+        L.icon_rows_forward.argtypes = [P, V, V, I, V]
+        L.icon_prepare_rhs.argtypes = [P, V, V, I, V]
+        L.icon_solve.argtypes = [P, ctypes.POINTER(SolveCfg), V, V, I, I, V, V, V]
+        L.icon_reproject.argtypes = [P, V, F, V, I, V]
+        L.icon_reconstruct_host.argtypes = [P, ctypes.POINTER(SolveCfg), V, V, V, I, V]
+        L.icon_trace_enable.argtypes = [P, I]
+        L.icon_trace_read.argtypes = [P, V, V, V]
+        L.icon_launch_count.argtypes = [P]
+        L.icon_launch_count.restype = ctypes.c_longlong
+        L.icon_last_error.restype = ctypes.c_char_p
+        for name in ("icon_plan_create", "icon_plan_destroy", "icon_plan_query", "icon_plan_geometry",
+                     "icon_nufft_forward", "icon_nufft_forward_complex", "icon_nufft_adjoint",
+                     "icon_rows_forward", "icon_prepare_rhs", "icon_solve", "icon_reproject",
+                     "icon_reconstruct_host", "icon_trace_enable", "icon_trace_read"):
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+class Geometry(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("thickness", ctypes.c_int), ("ntilt", ctypes.c_int),
+                ("tilt_deg", ctypes.POINTER(ctypes.c_float)), ("capacity", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+class SolveCfg(ctypes.Structure):
+    _fields_ = [("infr_before", ctypes.c_int), ("icon", ctypes.c_int), ("infr_after", ctypes.c_int),
+                ("data_type", ctypes.c_int), ("threshold", ctypes.c_float)]
+
+
+def _check(rc):
+    if rc != 0:
+        msg = lib().icon_last_error().decode(errors="replace")
+        raise IconError(f"icon status {rc}: {msg}")
+
+
+def _stream():
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class IconPlan:
+    """Plan for one tilt series: nx detector pixels, `thickness` (0 = nx)
+    reconstruction rows, tilt angles as in the .tlt file, up to `capacity`
+    slices per call."""
+
+    def __init__(self, nx, thickness, tilts, capacity=8, device=None):
+        import torch
+        if device is None:
+            device = torch.cuda.current_device()
+        self.device = torch.device("cuda", device)
+        self.tilts = np.ascontiguousarray(np.asarray(tilts, np.float32))
+        g = Geometry(int(nx), int(thickness), len(self.tilts),
+                     self.tilts.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(capacity), int(device))
+        h = ctypes.c_void_p()
+        _check(lib().icon_plan_create(ctypes.byref(g), ctypes.byref(h)))
+        self._h = h
+        d = (ctypes.c_int * 10)()
+        _check(lib().icon_plan_query(h, d))
+        self.N0, self.N1, self.n0, self.n1, self.M, self.nz, self.B, self.capacity, self.mib, self.omit_index = list(d)
+        self.nx = self.N0
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().icon_plan_destroy(h)
+            self._h = None
+
+    __del__ = close
+
+    def geometry(self):
+        xy = np.zeros((self.M, 2), np.float32)
+        w = np.zeros(self.M, np.float32)
+        _check(lib().icon_plan_geometry(self._h, xy.ctypes.data_as(ctypes.c_void_p), w.ctypes.data_as(ctypes.c_void_p)))
+        return xy, w
+
+    def _dev(self, t, dtype):
+        import torch
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.device == self.device and t.dtype == dtype and t.is_contiguous()):
+            raise IconError(f"expected a contiguous {dtype} tensor on {self.device}")
+        return t
+
+    def nufft_forward(self, img):
+        """img (S, N0, N1) float32 or complex64 -> nodes (S, M) complex64."""
+        import torch
+        S = img.shape[0]
+        out = torch.empty((S, self.M), dtype=torch.complex64, device=self.device)
+        if img.dtype == torch.complex64:
+            _check(lib().icon_nufft_forward_complex(self._h, _ptr(self._dev(img, torch.complex64)), _ptr(out), S, _stream()))
+        else:
+            _check(lib().icon_nufft_forward(self._h, _ptr(self._dev(img, torch.float32)), _ptr(out), S, _stream()))
+        return out
+
+    def nufft_adjoint(self, f):
+        """f (S, M) complex64 -> image (S, N0, N1) complex64."""
+        import torch
+        S = f.shape[0]
+        out = torch.empty((S, self.N0, self.N1), dtype=torch.complex64, device=self.device)
+        _check(lib().icon_nufft_adjoint(self._h, _ptr(self._dev(f, torch.complex64)), _ptr(out), S, _stream()))
+        return out
+
+    def rows_forward(self, rows):
+        """rows (S, nz, nx) float32 -> b (S, M) complex64."""
+        import torch
+        S = rows.shape[0]
+        out = torch.empty((S, self.M), dtype=torch.complex64, device=self.device)
+        _check(lib().icon_rows_forward(self._h, _ptr(self._dev(rows, torch.float32)), _ptr(out), S, _stream()))
+        return out
+
+    def prepare_rhs(self, rows):
+        """rows (S, nz, nx) float32 -> A^H W b (S, N0, N1) complex64."""
+        import torch
+        S = rows.shape[0]
+        out = torch.empty((S, self.N0, self.N1), dtype=torch.complex64, device=self.device)
+        _check(lib().icon_prepare_rhs(self._h, _ptr(self._dev(rows, torch.float32)), _ptr(out), S, _stream()))
+        return out
+
+    def solve(self, Ahwb, iters=(0, 10, 0), data_type=1, threshold=0.03, m0=None, history=False):
+        """Iteration3 on S slices; returns m (S, N0, N1) float32 (and, with
+        history=True, alpha and ||rhat||^2 per iteration as (iters, S))."""
+        import torch
+        S = Ahwb.shape[0]
+        a, b, c = iters
+        cfg = SolveCfg(int(a), int(b), int(c), int(data_type), float(threshold))
+        if m0 is None:
+            m = torch.empty((S, self.N0, self.N1), dtype=torch.float32, device=self.device)
+            warm = 0
+        else:
+            m = self._dev(m0, torch.float32).clone()
+            warm = 1
+        n = a + b + c
+        ha = np.zeros((max(n, 1), S), np.float64) if history else None
+        hr = np.zeros((max(n, 1), S), np.float64) if history else None
+        _check(lib().icon_solve(self._h, ctypes.byref(cfg), _ptr(self._dev(Ahwb, torch.complex64)), _ptr(m), S, warm,
+                                ha.ctypes.data_as(ctypes.c_void_p) if history else None,
+                                hr.ctypes.data_as(ctypes.c_void_p) if history else None, _stream()))
+        if history:
+            return m, ha[:n], hr[:n]
+        return m
+
+    def reproject(self, m, tilt_deg=None):
+        """m (S, N0, N1) float32 -> (S, nx) float32 reprojection at tilt_deg
+        (.tlt value; default the smallest-|angle| tilt, as Lib_2D2 does)."""
+        import torch
+        S = m.shape[0]
+        if tilt_deg is None:
+            tilt_deg = float(self.tilts[self.omit_index])
+        out = torch.empty((S, self.nx), dtype=torch.float32, device=self.device)
+        _check(lib().icon_reproject(self._h, _ptr(self._dev(m, torch.float32)), ctypes.c_float(tilt_deg), _ptr(out), S, _stream()))
+        return out
+
+    def reconstruct_host(self, rows, iters=(0, 10, 0), data_type=1, threshold=0.03, reproject=False, out=None,
+                         stream=None):
+        """Host arrays in and out: rows (S, nz, nx) float32 -> m (S, N0, N1)
+        (and the reprojection (S, nx) when reproject=True).  rows/out may be
+        numpy arrays or CPU torch tensors (pinned for full copy speed)."""
+        import torch
+        if isinstance(rows, torch.Tensor):
+            assert rows.device.type == "cpu" and rows.dtype == torch.float32 and rows.is_contiguous()
+            rptr, S = ctypes.c_void_p(rows.data_ptr()), rows.shape[0]
+        else:
+            r = np.ascontiguousarray(rows, np.float32)
+            rptr, S = r.ctypes.data_as(ctypes.c_void_p), r.shape[0]
+        if out is None:
+            out = np.empty((S, self.N0, self.N1), np.float32)
+        mptr = ctypes.c_void_p(out.data_ptr()) if isinstance(out, torch.Tensor) else out.ctypes.data_as(ctypes.c_void_p)
+        rp = np.empty((S, self.nx), np.float32) if reproject else None
+        a, b, c = iters
+        cfg = SolveCfg(int(a), int(b), int(c), int(data_type), float(threshold))
+        st = ctypes.c_void_p(stream) if stream is not None else None
+        _check(lib().icon_reconstruct_host(self._h, ctypes.byref(cfg), rptr, mptr,
+                                           rp.ctypes.data_as(ctypes.c_void_p) if reproject else None, S, st))
+        return (out, rp) if reproject else out
+
+    TRACE_KINDS = ("xpass_fwd", "ypass_fwd", "interp_fin", "ypass_adj", "xpass_adj", "alpha", "update", "rows_fwd",
+                   "layout", "row_adj")
+
+    def trace(self, enable=True):
+        _check(lib().icon_trace_enable(self._h, int(bool(enable))))
+
+    def trace_read(self):
+        """{kernel kind: (launches, total ms, algorithmic bytes)} since the last read."""
+        cnt = (ctypes.c_int * 10)()
+        ms = (ctypes.c_double * 10)()
+        by = (ctypes.c_double * 10)()
+        _check(lib().icon_trace_read(self._h, ctypes.cast(cnt, ctypes.c_void_p), ctypes.cast(ms, ctypes.c_void_p),
+                                     ctypes.cast(by, ctypes.c_void_p)))
+        return {k: (int(cnt[i]), float(ms[i]), float(by[i])) for i, k in enumerate(self.TRACE_KINDS)}
+
+    def launch_count(self):
+        return int(lib().icon_launch_count(self._h))

@@ -69,7 +69,7 @@ def tilt_angles(lo=-60.0, hi=60.0, step=2.0) -> np.ndarray:
     return (lo + step * np.arange(n)).astype(np.float32)
 
 
-def project(ph: Phantom, tilts_deg, ys=None, device="cpu", chunk=64) -> torch.Tensor:
+def project(ph: Phantom, tilts_deg, ys=None, device="cpu", chunk=16) -> torch.Tensor:
     """Clean projections rows[s, i, k] = line integral at tilt i, detector
     pixel k, of volume slice ys[s].  Returns float32 (S, ntilt, nx)."""
     nx, ny, nz = ph.shape

@@ -134,9 +134,26 @@ icon_status icon_reproject(icon_plan *plan, const float *d_m, float tilt_deg, fl
 /* The whole per-slice pipeline of Lib_2D2 (MainCode.cu:113-142) for S
  * slices from host memory: rows in, reconstructed slices out, plus the
  * reprojection at the smallest-|angle| tilt when h_reproj is not NULL.
- * Copies in and out through pinned staging buffers; synchronises. */
+ * Host buffers should be pinned for full copy speed.  Work is queued on
+ * `stream` (NULL: a stream of its own); the call returns after the results
+ * are in host memory.  S may exceed the capacity: it is processed in chunks. */
 icon_status icon_reconstruct_host(icon_plan *plan, const icon_solve_cfg *cfg, const float *h_rows, float *h_m,
-                                  float *h_reproj, int S);
+                                  float *h_reproj, int S, void *stream);
+
+/* Kernel tracing (no reference counterpart; the reference's cudaEvent timing
+ * blocks are commented out, e.g. Iteration2.cu:36-40).  While enabled, every
+ * kernel launch of the solver is bracketed by CUDA events on its stream.
+ * icon_trace_read synchronises, and for each of the ICON_TRACE_KERNELS kernel
+ * kinds returns the number of launches, their summed device time in ms and,
+ * when h_bytes is not NULL, their summed algorithmic bytes (the data each
+ * launch must read and write at least once), then clears the record.  Kinds, in order: xpass_fwd, ypass_fwd, interp_fin,
+ * ypass_adj, xpass_adj, alpha, update, rows_fwd, layout, row_adj. */
+#define ICON_TRACE_KERNELS 10
+icon_status icon_trace_enable(icon_plan *plan, int enable);
+icon_status icon_trace_read(icon_plan *plan, int *h_count, double *h_ms, double *h_bytes);
+
+/* Number of kernels this plan has launched since it was created. */
+long long icon_launch_count(const icon_plan *plan);
 
 /* Message for the last failed call on this thread ("" if none). */
 const char *icon_last_error(void);

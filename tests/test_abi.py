@@ -1,0 +1,50 @@
+"""CPU checks of the native boundary: the library builds for sm_100a, loads
+without a GPU, and exports every function include/*.h declares."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+
+def _declared_functions():
+    names = []
+    inc = os.path.join(ROOT, "include")
+    for fn in sorted(os.listdir(inc)):
+        if not fn.endswith(".h"):
+            continue
+        src = open(os.path.join(inc, fn)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?[a-z_]+\s*\*?\s*(icon_[a-z0-9_]+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = _declared_functions()
+    for n in ("icon_plan_create", "icon_nufft_forward", "icon_nufft_adjoint", "icon_solve", "icon_last_error"):
+        assert n in names
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    from feilab_b200 import build
+    lib_path = build.build_lib()
+    L = ctypes.CDLL(lib_path)
+    missing = [n for n in _declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+    L.icon_last_error.restype = ctypes.c_char_p
+    assert L.icon_last_error() == b""
+
+
+def test_plan_create_without_gpu_fails_cleanly():
+    # With no device the call must return an error status, not abort.
+    import torch
+    if torch.cuda.is_available():
+        return
+    from feilab_b200 import icon
+    import numpy as np
+    try:
+        icon.IconPlan(16, 16, np.array([-10, 0, 10], np.float32), capacity=1, device=0)
+    except icon.IconError as e:
+        assert "status" in str(e)
+    else:
+        raise AssertionError("plan creation without a GPU should fail")
