@@ -305,6 +305,26 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_profile_case(args):
+    """Small case for ncu captures: 16 slices of the workload (inputs and
+    intermediates of each kernel > L2, a few hundred MB on the device), the
+    input stage and 2 iterations; prints the traced kernel times."""
+    import torch
+    from feilab_b200 import icon
+    torch.cuda.set_device(0)
+    S = 16
+    rows, tilts = make_rows(list(range(S)), "cuda")
+    plan = icon.IconPlan(NX, THICK, tilts, capacity=S)
+    plan.trace(True)
+    A = plan.prepare_rhs(rows)
+    plan.solve(A, (0, 2, 0), DATA_TYPE, THRESHOLD)
+    torch.cuda.synchronize()
+    for k, v in plan.trace_read().items():
+        if v[0]:
+            print(f"{k:12s} launches {v[0]:4d}  ms {v[1]:9.3f}  algorithmic GB/s {v[2] / (v[1] / 1e3) / 1e9 if v[2] else 0:8.1f}")
+    plan.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -312,7 +332,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--profile", action="store_true", help="run the small ncu case only")
     args = ap.parse_args()
+    if args.profile:
+        run_profile_case(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
