@@ -20,8 +20,8 @@ CLI = os.path.join(HERE, "icon-gpu")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
 
-LIB_SOURCES = ["icon_api.cu"]
-LIB_DEPS = ["icon_api.cu", "icon_kernels.cuh", "icon_device.cuh"]
+LIB_SOURCES = ["icon_api.cu", "icon_noalloc.cu"]
+LIB_DEPS = ["icon_api.cu", "icon_noalloc.cu", "icon_kernels.cuh", "icon_device.cuh"]
 CLI_SOURCES = ["icon_cli.cpp", "mrc_io.cpp"]
 
 

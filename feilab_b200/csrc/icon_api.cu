@@ -804,4 +804,8 @@ icon_status icon_trace_read(icon_plan *p, int *h_count, double *h_ms, double *h_
 
 long long icon_launch_count(const icon_plan *p) { return p ? p->launches : 0; }
 
+// Lets the other translation units of the library report through
+// icon_last_error().
+void icon_internal_set_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
 }  // extern "C"

@@ -155,6 +155,24 @@ icon_status icon_trace_read(icon_plan *plan, int *h_count, double *h_ms, double 
 /* Number of kernels this plan has launched since it was created. */
 long long icon_launch_count(const icon_plan *plan);
 
+/* icon_rows_forward_noalloc: the work of icon_rows_forward (the 1-D NUFFT of
+ * every projection row, d_b[S][ntilt*nx] complex) for callers that cannot
+ * allocate device memory -- a process whose own pool allocator owns all
+ * device memory, or a real-time loop that must not call cudaMalloc because it
+ * can block on the device -- and so cannot create a plan.  No counterpart in
+ * the reference.  It calls no cudaMalloc, cudaFree or allocating library
+ * routine: its tables live in one file-scope __device__ array of
+ * ICON_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until
+ * the process exits.  nx must be in [8, ICON_NOALLOC_MAX_NX] (larger sizes
+ * return ICON_ERR_INVALID).  Runs on the current device and on `stream`.  The
+ * first call on a device looks up the array's device address and sets a
+ * kernel attribute, so make that first call before any stream capture.  All
+ * calls share the array: calls that overlap on one GPU (other streams or host
+ * threads) race on it and must be serialised by the caller. */
+#define ICON_NOALLOC_MAX_NX 4096
+#define ICON_NOALLOC_SCRATCH_BYTES (512 * 1024)
+icon_status icon_rows_forward_noalloc(const float *d_rows, int nx, int ntilt, int S, void *d_b, void *stream);
+
 /* Message for the last failed call on this thread ("" if none). */
 const char *icon_last_error(void);
 
