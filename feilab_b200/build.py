@@ -20,8 +20,12 @@ CLI = os.path.join(HERE, "icon-gpu")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
 
-LIB_SOURCES = ["icon_api.cu", "icon_noalloc.cu"]
-LIB_DEPS = ["icon_api.cu", "icon_noalloc.cu", "icon_kernels.cuh", "icon_device.cuh"]
+# (source, extra flags, object): the batched FFT kernels are built once per
+# slice-group size B, in parallel.
+LIB_UNITS = [("icon_api.cu", [], "icon_api.o"), ("icon_noalloc.cu", [], "icon_noalloc.o")] + [
+    ("icon_kern_b.cu", ["-DICON_KB=%d" % b], "icon_kern_b%d.o" % b) for b in (1, 2, 4, 8)]
+LIB_DEPS = ["icon_api.cu", "icon_noalloc.cu", "icon_kern_b.cu", "icon_launch.h", "icon_kernels.cuh", "icon_device.cuh"]
+BUILD_DIR = os.path.join(HERE, "_build")
 CLI_SOURCES = ["icon_cli.cpp", "mrc_io.cpp"]
 
 
@@ -43,10 +47,20 @@ def build_lib(force=False, verbose=False):
     deps = [os.path.join(CSRC, f) for f in LIB_DEPS] + [os.path.join(ROOT, "include", "icon_b200.h")]
     if not force and not _stale(LIB, deps):
         return LIB
-    cmd = [_nvcc(), *ARCH, *NVFLAGS, "-shared", "-o", LIB] + [os.path.join(CSRC, f) for f in LIB_SOURCES]
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    cmds = [[_nvcc(), *ARCH, *NVFLAGS, *extra, "-c", "-o", os.path.join(BUILD_DIR, obj), os.path.join(CSRC, src)]
+            for src, extra, obj in LIB_UNITS]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        for c in cmds:
+            print(" ".join(c))
+    procs = [subprocess.Popen(c) for c in cmds]
+    rcs = [p.wait() for p in procs]
+    if any(rcs):
+        raise subprocess.CalledProcessError(max(rcs), "nvcc")
+    link = [_nvcc(), *ARCH, "-shared", "-o", LIB] + [os.path.join(BUILD_DIR, obj) for _, _, obj in LIB_UNITS]
+    if verbose:
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     return LIB
 
 

@@ -17,6 +17,7 @@
 
 #include "icon_b200.h"
 #include "icon_kernels.cuh"
+#include "icon_launch.h"
 
 using icon::Geo;
 using icon::Geo1;
@@ -162,6 +163,7 @@ struct NodeTables {
     int M = 0;
     float *phix = nullptr, *phiy = nullptr, *w = nullptr;
     int *ix0 = nullptr, *iy0 = nullptr, *row_off = nullptr, *ent_jt = nullptr, *ent_iy0 = nullptr;
+    unsigned short *ent_lb = nullptr;
 };
 
 }  // namespace
@@ -173,9 +175,10 @@ struct icon_plan {
     float th0 = 0, th1 = 0, b0 = 0, bf0 = 0, b1 = 0, bf1 = 0;
     std::vector<float> tlt, th_neg, xy, w;
     int omit_index = 0;
+    float reproj_deg = 0.f;   // angle of icon_reconstruct_host's reprojection
     Arena arena;
     NodeTables nodes;
-    float *cx = nullptr, *cy = nullptr, *phi1 = nullptr;
+    float *cx = nullptr, *cy = nullptr, *rcx = nullptr, *rcy = nullptr, *phi1 = nullptr;
     int *i10 = nullptr;
     float2 *tw0 = nullptr, *tw1 = nullptr;
     // scratch sized for Gcap groups
@@ -186,8 +189,8 @@ struct icon_plan {
     // reprojection lines, keyed by the .tlt angle
     std::map<float, std::unique_ptr<NodeTables>> lines;
     float2 *fline = nullptr;
-    size_t smem_x = 0, smem_y = 0;
-    int thr_x = 0, thr_y = 0;
+    size_t smem_x = 0, smem_y = 0, smem_ya = 0;
+    int thr_x = 0, thr_y = 0, ex = 16, ey = 16;   // threads and values per thread of x- and y-pass FFTs
     // tracing: events around every launch while enabled
     bool trace = false;
     long long launches = 0;
@@ -224,7 +227,8 @@ struct icon_plan {
         g.N0 = N0; g.N1 = N1; g.n0 = n0; g.n1 = n1; g.lg0 = lg0; g.lg1 = lg1;
         g.M = t.M; g.nx = nx; g.nz = nz; g.B = B;
         g.w = t.w; g.phix = t.phix; g.phiy = t.phiy; g.ix0 = t.ix0; g.iy0 = t.iy0;
-        g.cx = cx; g.cy = cy; g.row_off = t.row_off; g.ent_jt = t.ent_jt; g.ent_iy0 = t.ent_iy0;
+        g.cx = cx; g.cy = cy; g.rcx = rcx; g.rcy = rcy; g.row_off = t.row_off; g.ent_jt = t.ent_jt; g.ent_iy0 = t.ent_iy0;
+        g.ent_lb = t.ent_lb;
         g.tw0 = tw0; g.tw1 = tw1;
         return g;
     }
@@ -261,6 +265,22 @@ enum Kind { K_XF = 0, K_YF, K_FIN, K_YA, K_XA, K_ALPHA, K_UPD, K_ROWS, K_LAYOUT,
     } while (0)
 #define LAUNCH(p, kind, st, ...) LAUNCH_B(p, kind, st, 0.0, __VA_ARGS__)
 
+// Runs the statement with L = the launcher class of the plan's B.
+#define WITH_B(Bv, ...)                                                  \
+    switch (Bv) {                                                        \
+    case 1: { using L = icon::Launch<1>; __VA_ARGS__; } break;           \
+    case 2: { using L = icon::Launch<2>; __VA_ARGS__; } break;           \
+    case 4: { using L = icon::Launch<4>; __VA_ARGS__; } break;           \
+    default: { using L = icon::Launch<8>; __VA_ARGS__; } break;          \
+    }
+
+// Shared-memory bytes of a rotated y-pass row buffer.
+inline size_t ybuf_bytes(int n1, int B)
+{
+    int sb = B == 8 ? 10 : (B == 4 ? 6 : B);
+    return (size_t)(n1 + 2 * icon::kHalo) * sb * sizeof(float2);
+}
+
 struct DeviceGuard {
     int prev = -1;
     bool ok = true;
@@ -284,12 +304,12 @@ icon_status build_tables(icon_plan *p, const float *xy, const float *w, int M, N
     float *xy_d = nullptr;
     ICON_TRY(p->arena.upload(&xy_d, xy, (size_t)2 * M));
     ICON_TRY(p->arena.alloc(&t.phix, (size_t)M * kTaps));
-    ICON_TRY(p->arena.alloc(&t.phiy, (size_t)M * kTaps));
+    ICON_TRY(p->arena.alloc(&t.phiy, (size_t)M * icon::kLdPhiy));
     ICON_TRY(p->arena.alloc(&t.ix0, (size_t)M));
     ICON_TRY(p->arena.alloc(&t.iy0, (size_t)M));
     int blk = 256, grd = (M + blk - 1) / blk;
-    icon::k_window<<<grd, blk>>>(xy_d, 2, M, p->n0, p->b0, p->bf0, t.phix, t.ix0);
-    icon::k_window<<<grd, blk>>>(xy_d + 1, 2, M, p->n1, p->b1, p->bf1, t.phiy, t.iy0);
+    icon::k_window<<<grd, blk>>>(xy_d, 2, M, p->n0, p->b0, p->bf0, t.phix, kTaps, t.ix0);
+    icon::k_window<<<grd, blk>>>(xy_d + 1, 2, M, p->n1, p->b1, p->bf1, t.phiy, icon::kLdPhiy, t.iy0);
     ICON_CUDA(cudaGetLastError());
     std::vector<int> ix0(M), iy0(M);
     ICON_CUDA(cudaMemcpy(ix0.data(), t.ix0, sizeof(int) * M, cudaMemcpyDeviceToHost));
@@ -325,9 +345,25 @@ icon_status build_tables(icon_plan *p, const float *xy, const float *w, int M, N
             ky2[a + i] = ky[order[i]];
         }
     }
+    // Per row, the entries whose first rotated y tap r0 = iy0 + n1/2 + 8 is
+    // below v (v = 0..n1+16), relative to the row's first entry.
+    const int ldl = icon::lb_ld(p->n1), r0ofs = p->n1 / 2 + icon::kHalo;
+    std::vector<unsigned short> lb((size_t)n0 * ldl);
+    for (int x = 0; x < n0; ++x) {
+        int a = cnt[x], c = cnt[x + 1];
+        if (c - a > 65535) return fail(ICON_ERR_INVALID, "more than 65535 window entries on one grid row");
+        int e = a;
+        for (int v = 0; v < ldl; ++v) {
+            while (e < c && ky2[e] + r0ofs < v) ++e;
+            lb[(size_t)x * ldl + v] = (unsigned short)(e - a);
+        }
+        if (c > a && (ky2[a] + r0ofs < 0 || ky2[c - 1] + r0ofs + kTaps > ldl - 1))
+            return fail(ICON_ERR_INVALID, "window taps outside the rotated y buffer");
+    }
     ICON_TRY(p->arena.upload(&t.row_off, cnt.data(), (size_t)n0 + 1));
     ICON_TRY(p->arena.upload(&t.ent_jt, jt2.data(), E));
     ICON_TRY(p->arena.upload(&t.ent_iy0, ky2.data(), E));
+    ICON_TRY(p->arena.upload(&t.ent_lb, lb.data(), lb.size()));
     ICON_TRY(p->arena.upload(&t.w, w, (size_t)M));
     return ICON_OK;
 }
@@ -377,14 +413,15 @@ icon_status launch_forward(icon_plan *p, const NodeTables &t, const void *img_in
     const StageBytes sb = stage_bytes(p, t);
     const double slots = (double)G * p->B;
     dim3 gx(p->N1, G), gy(p->n0, G);
-    if (real_in) LAUNCH_B(p, K_XF, st, sb.xf_real * slots, icon::k_xpass_fwd<true><<<gx, p->thr_x, p->smem_x, st>>>(g, img_int, p->G1));
-    else LAUNCH_B(p, K_XF, st, sb.xf_cplx * slots, icon::k_xpass_fwd<false><<<gx, p->thr_x, p->smem_x, st>>>(g, img_int, p->G1));
-    LAUNCH_B(p, K_YF, st, sb.yf * slots, icon::k_ypass_fwd<<<gy, p->thr_y, p->smem_y, st>>>(g, p->G1, p->P));
+    WITH_B(p->B,
+        LAUNCH_B(p, K_XF, st, (real_in ? sb.xf_real : sb.xf_cplx) * slots,
+                 L::xpass_fwd(real_in, p->ex, gx, p->thr_x, p->smem_x, st, g, img_int, p->G1));
+        LAUNCH_B(p, K_YF, st, sb.yf * slots, L::ypass_fwd(p->ey, gy, p->thr_y, p->smem_y, st, g, p->G1, p->P)))
     int kb = (t.M * p->B + 255) / 256;
     dim3 g3(kb, G);
-    if (mode == 0) LAUNCH_B(p, K_FIN, st, sb.fin_store * slots, icon::k_interp_fin<0><<<g3, 256, 0, st>>>(g, p->P, f_out, nullptr));
-    else if (mode == 1) LAUNCH_B(p, K_FIN, st, sb.fin_store * slots, icon::k_interp_fin<1><<<g3, 256, 0, st>>>(g, p->P, f_out, nullptr));
-    else LAUNCH_B(p, K_FIN, st, sb.fin_red * slots, icon::k_interp_fin<2><<<g3, 256, 0, st>>>(g, p->P, nullptr, p->part_rtar));
+    WITH_B(p->B,
+        LAUNCH_B(p, K_FIN, st, (mode == 2 ? sb.fin_red : sb.fin_store) * slots,
+                 L::interp_fin(mode, g3, st, g, p->P, mode == 2 ? nullptr : f_out, mode == 2 ? p->part_rtar : nullptr)))
     ICON_CUDA(cudaGetLastError());
     return ICON_OK;
 }
@@ -395,10 +432,12 @@ icon_status launch_adjoint(icon_plan *p, const float2 *f_int, int G, int mode, f
     const StageBytes sb = stage_bytes(p, p->nodes);
     const double slots = (double)G * p->B;
     dim3 gy(p->n0, G), gx(p->N1, G);
-    LAUNCH_B(p, K_YA, st, sb.ya * slots, icon::k_ypass_adj<<<gy, p->thr_y, p->smem_y, st>>>(g, f_int, p->G1));
     size_t smem = p->smem_x + sizeof(double) * p->thr_x;
-    if (mode == 0) LAUNCH_B(p, K_XA, st, sb.xa_plain * slots, icon::k_xpass_adj<0><<<gx, p->thr_x, smem, st>>>(g, p->G1, out_int, nullptr, nullptr));
-    else LAUNCH_B(p, K_XA, st, sb.xa_resid * slots, icon::k_xpass_adj<1><<<gx, p->thr_x, smem, st>>>(g, p->G1, out_int, p->Ahwb, p->part_rtr));
+    WITH_B(p->B,
+        LAUNCH_B(p, K_YA, st, sb.ya * slots, L::ypass_adj(p->ey, gy, p->thr_y, p->smem_ya, st, g, f_int, p->G1));
+        LAUNCH_B(p, K_XA, st, (mode == 0 ? sb.xa_plain : sb.xa_resid) * slots,
+                 L::xpass_adj(mode, p->ex, gx, p->thr_x, smem, st, g, p->G1, out_int, mode == 0 ? nullptr : p->Ahwb,
+                              mode == 0 ? nullptr : p->part_rtr)))
     ICON_CUDA(cudaGetLastError());
     return ICON_OK;
 }
@@ -406,7 +445,7 @@ icon_status launch_adjoint(icon_plan *p, const float2 *f_int, int G, int mode, f
 icon_status launch_rows(icon_plan *p, const float *d_rows, int S, int G, float2 *bout, cudaStream_t st)
 {
     Geo g = p->geo(p->nodes);
-    LAUNCH(p, K_ROWS, st, icon::k_rows_fwd<<<dim3(p->nz, G), p->thr_x, p->smem_x, st>>>(g, p->geo1(), d_rows, S, p->f, bout));
+    WITH_B(p->B, LAUNCH(p, K_ROWS, st, L::rows_fwd(p->ex, dim3(p->nz, G), p->thr_x, p->smem_x, st, g, p->geo1(), d_rows, S, p->f, bout)))
     ICON_CUDA(cudaGetLastError());
     return ICON_OK;
 }
@@ -420,9 +459,10 @@ icon_status launch_iteration(icon_plan *p, int G, bool clamp, int data_type, flo
     ICON_TRY(launch_forward(p, p->nodes, p->rhat, false, G, 2, nullptr, st));   // r = A rhat, sum w|r|^2
     int kb = (p->M * p->B + 255) / 256;
     LAUNCH(p, K_ALPHA, st, icon::k_alpha<<<G, 32 * p->B, 0, st>>>(p->part_rtr, p->N1, p->part_rtar, kb, p->B, p->alpha, hist_a, hist_r));
-    size_t per_group = (size_t)p->N1 * p->N0 * p->B, total = per_group * G;
-    LAUNCH_B(p, K_UPD, st, stage_bytes(p, p->nodes).upd * G * p->B, icon::k_update<<<grid1d(total), 256, 0, st>>>(p->m, p->rhat, p->alpha, p->B, per_group, total,
-                                                                       clamp ? 1 : 0, data_type, thr));
+    int per_group = p->N1 * p->N0 * p->B;
+    dim3 gu((unsigned)std::min<size_t>(((size_t)per_group + 255) / 256, 512), G);
+    WITH_B(p->B, LAUNCH_B(p, K_UPD, st, stage_bytes(p, p->nodes).upd * G * p->B,
+                          L::update(gu, st, p->m, p->rhat, p->alpha, per_group, clamp ? 1 : 0, data_type, thr)))
     ICON_CUDA(cudaGetLastError());
     return ICON_OK;
 }
@@ -451,7 +491,7 @@ icon_status reproject_internal(icon_plan *p, const float *m_int, float tilt_deg,
     int G = groups(p, S);
     ICON_TRY(launch_forward(p, *lt, m_int, true, G, 0, p->fline, st));
     Geo g = p->geo(*lt);
-    LAUNCH(p, K_ROWADJ, st, icon::k_row_adj<<<G, p->thr_x, p->smem_x, st>>>(g, p->geo1(), p->fline, d_out, S));
+    WITH_B(p->B, LAUNCH(p, K_ROWADJ, st, L::row_adj(p->ex, dim3(G), p->thr_x, p->smem_x, st, g, p->geo1(), p->fline, d_out, S)))
     ICON_CUDA(cudaGetLastError());
     return ICON_OK;
 }
@@ -462,6 +502,25 @@ icon_status reproject_internal(icon_plan *p, const float *m_int, float tilt_deg,
 extern "C" {
 
 const char *icon_last_error(void) { return g_last_error.c_str(); }
+
+icon_status icon_devices(int *h_count, int *h_sm, int max)
+{
+    if (!h_count) return fail(ICON_ERR_INVALID, "null argument");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        *h_count = 0;
+        cudaGetLastError();
+        return fail(ICON_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+    }
+    *h_count = n;
+    for (int d = 0; h_sm && d < n && d < max; ++d) {
+        int sm = 0;
+        ICON_CUDA(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, d));
+        h_sm[d] = sm;
+    }
+    return ICON_OK;
+}
 
 icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
 {
@@ -506,6 +565,7 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
             om = p->th_neg[i];
             p->omit_index = i;
         }
+    p->reproj_deg = p->tlt[p->omit_index];
     p->xy.resize((size_t)2 * p->M);
     p->w.resize(p->M);
     px2d(nx, nz, p->th_neg.data(), p->xy.data());
@@ -514,6 +574,11 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
     std::vector<float> cx = deapod(p->N0, p->n0, p->b0), cy = deapod(p->N1, p->n1, p->b1);
     ICON_TRY(p->arena.upload(&p->cx, cx.data(), cx.size()));
     ICON_TRY(p->arena.upload(&p->cy, cy.data(), cy.size()));
+    std::vector<float> rcx(cx.size()), rcy(cy.size());
+    for (size_t i = 0; i < cx.size(); ++i) rcx[i] = (float)(1.0 / (double)cx[i]);
+    for (size_t i = 0; i < cy.size(); ++i) rcy[i] = (float)(1.0 / (double)cy[i]);
+    ICON_TRY(p->arena.upload(&p->rcx, rcx.data(), rcx.size()));
+    ICON_TRY(p->arena.upload(&p->rcy, rcy.data(), rcy.size()));
     // 1-D row transform nodes (k - nx/2)/nx (MainCode.cu:72-80).
     std::vector<float> px1((size_t)nx);
     for (int k = 0; k < nx; ++k) px1[k] = (float)(((double)(float)k - (double)(float)nx / 2.0) / (double)(float)nx);
@@ -521,28 +586,35 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
     ICON_TRY(p->arena.upload(&px1_d, px1.data(), px1.size()));
     ICON_TRY(p->arena.alloc(&p->phi1, (size_t)nx * kTaps));
     ICON_TRY(p->arena.alloc(&p->i10, (size_t)nx));
-    icon::k_window<<<(nx + 255) / 256, 256>>>(px1_d, 1, nx, p->n0, p->b0, p->bf0, p->phi1, p->i10);
+    icon::k_window<<<(nx + 255) / 256, 256>>>(px1_d, 1, nx, p->n0, p->b0, p->bf0, p->phi1, kTaps, p->i10);
     ICON_CUDA(cudaGetLastError());
     std::vector<float2> t0 = twiddles(p->n0), t1 = twiddles(p->n1);
     ICON_TRY(p->arena.upload(&p->tw0, t0.data(), t0.size()));
     ICON_TRY(p->arena.upload(&p->tw1, t1.data(), t1.size()));
-    // Launch shapes: one thread per 16 values of an [n][B] FFT buffer.
-    p->thr_x = p->n0 * B / 16;
-    p->thr_y = p->n1 * B / 16;
+    // Launch shapes: an FFT thread owns E values of an [n][B] batch: 32 when
+    // radix-32 passes need fewer passes than radix-16 ones and the block still
+    // has a full warp, else 16.
+    auto pick_e = [&](int lg, int n) {
+        bool fewer = (lg + 4) / 5 < (lg + 3) / 4;
+        return (fewer && n * B >= 32 * 32) ? 32 : 16;
+    };
+    p->ex = pick_e(p->lg0, p->n0);
+    p->ey = pick_e(p->lg1, p->n1);
+    p->thr_x = p->n0 * B / p->ex;
+    p->thr_y = p->n1 * B / p->ey;
     p->smem_x = (size_t)p->n0 * B * sizeof(float2);
-    p->smem_y = (size_t)p->n1 * B * sizeof(float2);
+    p->smem_y = ybuf_bytes(p->n1, B);
+    p->smem_ya = icon::ypass_adj_smem(p->n1, B);
     int smem_max = 0;
     ICON_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     size_t need_x = p->smem_x + sizeof(double) * p->thr_x;
-    if ((size_t)smem_max < std::max(need_x, p->smem_y)) return fail(ICON_ERR_INVALID, "FFT buffer exceeds shared memory");
-    ICON_CUDA(cudaFuncSetAttribute(icon::k_xpass_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_x));
-    ICON_CUDA(cudaFuncSetAttribute(icon::k_xpass_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_x));
-    ICON_CUDA(cudaFuncSetAttribute(icon::k_ypass_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_y));
-    ICON_CUDA(cudaFuncSetAttribute(icon::k_ypass_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_y));
-    ICON_CUDA(cudaFuncSetAttribute(icon::k_xpass_adj<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_x));
-    ICON_CUDA(cudaFuncSetAttribute(icon::k_xpass_adj<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_x));
-    ICON_CUDA(cudaFuncSetAttribute(icon::k_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_x));
-    ICON_CUDA(cudaFuncSetAttribute(icon::k_row_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_x));
+    if ((size_t)smem_max < std::max(need_x, std::max(p->smem_y, p->smem_ya)))
+        return fail(ICON_ERR_INVALID, "FFT buffer exceeds shared memory");
+    {
+        cudaError_t e = cudaSuccess;
+        WITH_B(B, e = L::set_smem(p->ex, p->ey, p->smem_x, need_x, p->smem_y, p->smem_ya))
+        if (e != cudaSuccess) return fail(ICON_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    }
     // Scratch for Gcap groups.
     size_t G = p->Gcap, Bz = B;
     ICON_TRY(p->arena.alloc(&p->G1, G * p->n0 * p->N1 * Bz));
@@ -572,6 +644,14 @@ icon_status icon_plan_destroy(icon_plan *plan)
     DeviceGuard guard(plan->dev);
     cudaDeviceSynchronize();
     delete plan;
+    return ICON_OK;
+}
+
+icon_status icon_plan_set_reprojection(icon_plan *p, float tilt_deg)
+{
+    if (!p) return fail(ICON_ERR_INVALID, "null plan");
+    if (!std::isfinite(tilt_deg)) return fail(ICON_ERR_INVALID, "angle must be finite");
+    p->reproj_deg = tilt_deg;
     return ICON_OK;
 }
 
@@ -751,7 +831,7 @@ icon_status icon_reconstruct_host(icon_plan *p, const icon_solve_cfg *cfg, const
             rc = launch_iteration(p, G, a <= it && it < iters - c, cfg->data_type, cfg->threshold, nullptr, nullptr, st);
         if (rc != ICON_OK) break;
         LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float><<<grid1d((size_t)Sc * NN), 256, 0, st>>>(p->m, d_mo, Sc, p->N0, p->N1, p->B));
-        if (h_reproj && (rc = reproject_internal(p, p->m, p->tlt[p->omit_index], p->outrp, Sc, st)) != ICON_OK) break;
+        if (h_reproj && (rc = reproject_internal(p, p->m, p->reproj_deg, p->outrp, Sc, st)) != ICON_OK) break;
         if ((e = cudaMemcpyAsync(h_m + (size_t)s0 * NN, d_mo, sizeof(float) * NN * Sc, cudaMemcpyDeviceToHost, st)) != cudaSuccess) {
             rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
             break;

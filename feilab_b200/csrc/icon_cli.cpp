@@ -1,0 +1,490 @@
+// icon_cli.cpp -- icon-gpu, a drop-in for the ICON-GPU v1.2.9 command-line
+// tool (ICON-GPU/ICONGPU.cu:93-609) on the B200 engine of libicon_b200.
+//
+// Same flags, spellings, defaults and exit behaviour (-1 on -help or a missing
+// parameter, ICONGPU.cu:283-316), same output files:
+//   <o>/reconstruction/mid%05d.mrc        one xz-slice per file, X fastest
+//                                         (saveMRC_real_inv, saveMRC_real.cu:33-56)
+//   <o>/crossValidation/GroundTruth.mrc, fullRec_reProjection.mrc,
+//   crossV_reprojection.mrc, fullRec.frc, crossV.frc   (ICONGPU.cu:468-592)
+// plus, with --volume FILE, the slices stacked into one MRC volume.
+// Slices are reconstructed in batches on each listed GPU; slice ranges are
+// split across GPUs in proportion to their SM counts (ICONGPU.cu:393-466).
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "icon_b200.h"
+#include "mrc_io.h"
+
+namespace {
+
+void help()
+{
+    printf("ICON parameter\n######\n");
+    printf("-input (-i) : the aligned tilt series.\n######\n");
+    printf("-tiltfile (-t) : the aligned tilt file.\n######\n");
+    printf("-outputPath (-o) : the folder for the results; \"crossValidation\" and \"reconstruction\" are created inside.\n######\n");
+    printf("-slice (-s) : first and last slice, split by ','. For example 0,511 reconstructs slices 0 to 511.\n######\n");
+    printf("-ICONIteration (-iter) : iterations a,b,c: a INFR iterations, b ICON iterations, c INFR iterations.\n######\n");
+    printf("-dataType (-d) : 1 for cryoET or plastic embedded ET (signal black), 2 for negative stain (signal white); default 1.\n######\n");
+    printf("-threshold (-thr) : the threshold used in ICON, default 0.03 (-0.03 for data type 2).\n######\n");
+    printf("-skipCrossValidation (-skipCV) : 1 skips the cross validation and its frc files; default 0.\n######\n");
+    printf("-gpu (-g) : the GPUs to use, e.g. 0,2,4,6; default -1, all GPUs.\n######\n");
+    printf("-help (-h) : for help.\n");
+    printf("long options: --volume FILE (write the slices as one MRC volume), --batch N (slices per GPU batch)\n");
+}
+
+struct Args {
+    std::string input, tilt, out, volume;
+    int ystart = 0, yend = -1;
+    int iters[3] = {0, 0, 0};
+    int data_type = 1;
+    float threshold = 520.0f;
+    int thickness = 0;
+    int skip_cv = 0;
+    std::vector<int> gpus;
+    int batch = 64;
+};
+
+// Per-GPU work: a contiguous slice range.
+struct Job {
+    int device = 0;
+    int y0 = 0, y1 = 0;   // [y0, y1)
+    int rc = 0;
+    std::string err;
+};
+
+std::string join(const std::string &a, const std::string &b) { return a + "/" + b; }
+
+// 1-D DFT of any length (radix-2 for powers of two, Bluestein otherwise), in
+// double; used for the FRC of the cross-validation outputs.
+void fft_pow2(std::vector<std::complex<double>> &a, bool inverse)
+{
+    size_t n = a.size();
+    for (size_t i = 1, j = 0; i < n; ++i) {
+        size_t bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    for (size_t len = 2; len <= n; len <<= 1) {
+        double ang = 2 * M_PI / (double)len * (inverse ? 1 : -1);
+        for (size_t i = 0; i < n; i += len)
+            for (size_t k = 0; k < len / 2; ++k) {
+                std::complex<double> w = std::polar(1.0, ang * (double)k);
+                std::complex<double> u = a[i + k], v = a[i + k + len / 2] * w;
+                a[i + k] = u + v;
+                a[i + k + len / 2] = u - v;
+            }
+    }
+}
+
+void fft_any(std::vector<std::complex<double>> &a)
+{
+    size_t n = a.size();
+    if ((n & (n - 1)) == 0) {
+        fft_pow2(a, false);
+        return;
+    }
+    size_t m = 1;
+    while (m < 2 * n - 1) m <<= 1;
+    std::vector<std::complex<double>> w(n), x(m), y(m);
+    for (size_t k = 0; k < n; ++k) w[k] = std::polar(1.0, -M_PI * (double)((k * k) % (2 * n)) / (double)n);
+    for (size_t k = 0; k < n; ++k) x[k] = a[k] * w[k];
+    y[0] = std::conj(w[0]);
+    for (size_t k = 1; k < n; ++k) y[k] = y[m - k] = std::conj(w[k]);
+    fft_pow2(x, false);
+    fft_pow2(y, false);
+    for (size_t i = 0; i < m; ++i) x[i] *= y[i];
+    fft_pow2(x, true);
+    for (size_t k = 0; k < n; ++k) a[k] = x[k] * w[k] / (double)m;
+}
+
+// calFRC_nonsqure (calFRC.cu:93-174): 2-D FFT of two nx-by-ny images (nx
+// fastest), ring sums with the y frequency scaled by (nx/ny)^2, FRC per ring
+// r < nx/2, frc[0] = 1.
+std::vector<float> frc_nonsquare(const std::vector<float> &a, const std::vector<float> &b, int nx, int ny)
+{
+    auto fft2 = [&](const std::vector<float> &img) {
+        std::vector<std::complex<double>> f((size_t)nx * ny);
+        for (size_t i = 0; i < f.size(); ++i) f[i] = img[i];
+        std::vector<std::complex<double>> line(nx);
+        for (int j = 0; j < ny; ++j) {
+            for (int i = 0; i < nx; ++i) line[i] = f[(size_t)j * nx + i];
+            fft_any(line);
+            for (int i = 0; i < nx; ++i) f[(size_t)j * nx + i] = line[i];
+        }
+        std::vector<std::complex<double>> col(ny);
+        for (int i = 0; i < nx; ++i) {
+            for (int j = 0; j < ny; ++j) col[j] = f[(size_t)j * nx + i];
+            fft_any(col);
+            for (int j = 0; j < ny; ++j) f[(size_t)j * nx + i] = col[j];
+        }
+        return f;
+    };
+    std::vector<std::complex<double>> A = fft2(a), Bf = fft2(b);
+    int nx2 = nx / 2, ny2 = ny / 2;
+    std::vector<double> up(nx2 + 1, 0.0), l1(nx2 + 1, 0.0), l2(nx2 + 1, 0.0);
+    float damp = ((float)nx / (float)ny) * ((float)nx / (float)ny);
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            int i1 = (i + nx2) % nx, j1 = (j + ny2) % ny;
+            int r = (int)std::floor(std::sqrt((float)((i1 - nx2) * (i1 - nx2)) + (float)((j1 - ny2) * (j1 - ny2)) * damp));
+            if (r < nx2) {
+                std::complex<double> p = A[(size_t)j * nx + i], q = Bf[(size_t)j * nx + i];
+                up[r] += p.real() * q.real() + p.imag() * q.imag();
+                l1[r] += std::norm(p);
+                l2[r] += std::norm(q);
+            }
+        }
+    std::vector<float> frc(nx2 > 0 ? nx2 : 1, 0.f);
+    frc[0] = 1.f;
+    for (int i = 1; i < nx2; ++i) {
+        double d = std::sqrt(l1[i]) * std::sqrt(l2[i]);
+        frc[i] = d != 0 ? (float)(up[i] / d) : 0.f;
+    }
+    return frc;
+}
+
+// frcSmooth (ICONGPU.cu:59-91): moving average over `overlap` bins.
+void frc_smooth(std::vector<float> &frc, int size, int overlap)
+{
+    std::vector<float> t(size);
+    for (int i = 0; i < size; ++i) {
+        int jbe = i - overlap / 2;
+        if (jbe < 0) jbe = 0;
+        int jen = jbe + overlap;
+        if (jen > size - 1) {
+            jbe -= jen - size + 1;
+            jen = size - 1;
+        }
+        if (jbe < 0) jbe = 0;
+        float sum = 0;
+        int num = 0;
+        for (int j = jbe; j < jen; ++j) {
+            sum += frc[j];
+            ++num;
+        }
+        t[i] = num ? sum / num : 0.f;
+    }
+    for (int i = 0; i < size; ++i) frc[i] = t[i];
+}
+
+// One GPU's share: reconstruct slices [y0, y1) (and, unless skipped, the
+// cross-validation solve), write the slice files, fill the reprojections.
+void run_job(Job &job, const Args &A, const MrcHeader &inh, const std::vector<float> &tilts, int thickness,
+             const std::vector<float> &stack, int omit, std::vector<float> &rp_full, std::vector<float> &rp_cv,
+             std::vector<float> *volume, const std::string &recdir)
+{
+    const int nx = inh.nx, ny = inh.ny, nz = inh.nz;
+    const int S = job.y1 - job.y0;
+    if (S <= 0) return;
+    icon_solve_cfg cfg{A.iters[0], A.iters[1], A.iters[2], A.data_type, A.threshold};
+    const int cap = std::min(A.batch, S);
+    const size_t NN = (size_t)nx * thickness;
+    auto fail = [&](const std::string &m) {
+        job.rc = 1;
+        job.err = m + ": " + icon_last_error();
+    };
+    // Full reconstruction (Lib_2D2, MainCode.cu:3-177).
+    {
+        icon_geometry g{nx, thickness, nz, tilts.data(), cap, job.device};
+        icon_plan *plan = nullptr;
+        if (icon_plan_create(&g, &plan) != ICON_OK) return fail("plan");
+        std::vector<float> rows((size_t)cap * nz * nx), m((size_t)cap * NN), rp((size_t)cap * nx);
+        for (int s0 = 0; s0 < S; s0 += cap) {
+            int sc = std::min(cap, S - s0);
+            for (int s = 0; s < sc; ++s)
+                for (int i = 0; i < nz; ++i)
+                    std::memcpy(&rows[((size_t)s * nz + i) * nx], &stack[((size_t)i * ny + job.y0 + s0 + s) * nx],
+                                sizeof(float) * nx);
+            auto t0 = std::chrono::steady_clock::now();
+            if (icon_reconstruct_host(plan, &cfg, rows.data(), m.data(), rp.data(), sc, nullptr) != ICON_OK) {
+                icon_plan_destroy(plan);
+                return fail("reconstruction");
+            }
+            double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            std::vector<float> slice(NN);
+            for (int s = 0; s < sc; ++s) {
+                int y = job.y0 + s0 + s;
+                const float *ms = &m[(size_t)s * NN];
+                for (int j = 0; j < thickness; ++j)          // saveMRC_real_inv: X fastest
+                    for (int i = 0; i < nx; ++i) slice[(size_t)j * nx + i] = ms[(size_t)i * thickness + j];
+                MrcHeader oh = inh;                           // saveMRC_real.cu:37-46
+                oh.mz = inh.mx;
+                oh.zlen = inh.xlen;
+                oh.nx = nx;
+                oh.ny = thickness;
+                oh.nz = 1;
+                char name[64];
+                snprintf(name, sizeof name, "mid%05d.mrc", y);
+                std::string e;
+                if (!mrc_write_float(join(recdir, name), oh, slice.data(), e)) {
+                    icon_plan_destroy(plan);
+                    job.rc = 1;
+                    job.err = e;
+                    return;
+                }
+                if (volume) std::memcpy(&(*volume)[(size_t)(y - A.ystart) * NN], slice.data(), sizeof(float) * NN);
+                std::memcpy(&rp_full[(size_t)(y - A.ystart) * nx], &rp[(size_t)s * nx], sizeof(float) * nx);
+                printf("slice %d finished, time %lf\n", y, dt / sc);
+            }
+        }
+        icon_plan_destroy(plan);
+    }
+    if (A.skip_cv) return;
+    // Cross-validation solve without the smallest-|angle| tilt, reprojected
+    // at that tilt (Lib_2D_crossV2, MainCode_crossV.cu:3-189).
+    std::vector<float> t2;
+    for (int i = 0; i < nz; ++i)
+        if (i != omit) t2.push_back(tilts[i]);
+    icon_geometry g{nx, thickness, nz - 1, t2.data(), cap, job.device};
+    icon_plan *plan = nullptr;
+    if (icon_plan_create(&g, &plan) != ICON_OK) return fail("cross-validation plan");
+    if (icon_plan_set_reprojection(plan, tilts[omit]) != ICON_OK) {
+        icon_plan_destroy(plan);
+        return fail("cross-validation reprojection angle");
+    }
+    std::vector<float> rows((size_t)cap * (nz - 1) * nx), m((size_t)cap * NN), rp((size_t)cap * nx);
+    for (int s0 = 0; s0 < S; s0 += cap) {
+        int sc = std::min(cap, S - s0);
+        for (int s = 0; s < sc; ++s)
+            for (int i = 0, k = 0; i < nz; ++i) {
+                if (i == omit) continue;
+                std::memcpy(&rows[((size_t)s * (nz - 1) + k) * nx], &stack[((size_t)i * ny + job.y0 + s0 + s) * nx],
+                            sizeof(float) * nx);
+                ++k;
+            }
+        if (icon_reconstruct_host(plan, &cfg, rows.data(), m.data(), rp.data(), sc, nullptr) != ICON_OK) {
+            icon_plan_destroy(plan);
+            return fail("cross-validation reconstruction");
+        }
+        for (int s = 0; s < sc; ++s)
+            std::memcpy(&rp_cv[(size_t)(job.y0 + s0 + s - A.ystart) * nx], &rp[(size_t)s * nx], sizeof(float) * nx);
+    }
+    icon_plan_destroy(plan);
+}
+
+bool next_arg(int argc, char **argv, int &i, std::string &v)
+{
+    if (i + 1 >= argc) return false;
+    v = argv[++i];
+    ++i;
+    return true;
+}
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+    Args A;
+    bool mark[10] = {false, false, false, false, false, true, true, true, true, true};   // ICONGPU.cu:142-149
+    int ndev = 0;
+    std::vector<int> sm(256, 0);
+    icon_devices(&ndev, sm.data(), 256);
+    printf("##################\n%d GPU(s) are detected in the system!\n", ndev);
+    for (int d = 0; d < ndev; ++d) A.gpus.push_back(d);
+    int i = 1;
+    while (i < argc) {
+        std::string a = argv[i], v;
+        if (a.size() > 2 && a[0] == '-' && a[1] == '-') {               // long options of this tool
+            if (a == "--volume" && next_arg(argc, argv, i, v)) A.volume = v;
+            else if (a == "--batch" && next_arg(argc, argv, i, v)) A.batch = std::max(1, atoi(v.c_str()));
+            else if (a == "--help") { help(); return -1; }
+            else { printf("parameter error!\n Please use -help to see the manual\n"); return -1; }
+            continue;
+        }
+        if (a[0] != '-') { ++i; continue; }
+        std::string k = a.substr(1);
+        bool needs = (k == "input" || k == "i" || k == "tiltfile" || k == "t" || k == "outputPath" || k == "o" ||
+                      k == "slice" || k == "s" || k == "ICONIteration" || k == "iter" || k == "dataType" ||
+                      k == "d" || k == "threshold" || k == "thr" || k == "gpu" || k == "g" || k == "thickness" ||
+                      k == "thi" || k == "skipCrossValidation" || k == "skipCV");
+        if (k == "help" || k == "h") {
+            help();
+            return -1;
+        }
+        if (!needs) { ++i; continue; }
+        if (!next_arg(argc, argv, i, v)) { printf("parameter error!\n Please use -help to see the manual\n"); return -1; }
+        if (k == "input" || k == "i") { A.input = v; mark[0] = true; }
+        else if (k == "tiltfile" || k == "t") { A.tilt = v; mark[1] = true; }
+        else if (k == "outputPath" || k == "o") { A.out = v; mark[2] = true; }
+        else if (k == "slice" || k == "s") { if (sscanf(v.c_str(), "%d,%d", &A.ystart, &A.yend) == 2) mark[3] = true; }
+        else if (k == "ICONIteration" || k == "iter") {
+            if (sscanf(v.c_str(), "%d,%d,%d", &A.iters[0], &A.iters[1], &A.iters[2]) == 3) mark[4] = true;
+        }
+        else if (k == "dataType" || k == "d") A.data_type = atoi(v.c_str());
+        else if (k == "threshold" || k == "thr") A.threshold = (float)atof(v.c_str());
+        else if (k == "thickness" || k == "thi") A.thickness = atoi(v.c_str());
+        else if (k == "skipCrossValidation" || k == "skipCV") A.skip_cv = atoi(v.c_str());
+        else if (k == "gpu" || k == "g") {                             // ICONGPU.cu:231-263
+            std::vector<int> list;
+            size_t p = 0;
+            while (p <= v.size()) {
+                size_t q = v.find(',', p);
+                std::string tok = v.substr(p, q == std::string::npos ? std::string::npos : q - p);
+                int d = atoi(tok.c_str());
+                if (d == -1) break;
+                list.push_back(d);
+                if (q == std::string::npos) break;
+                p = q + 1;
+            }
+            if (!list.empty()) A.gpus = list;
+        }
+    }
+    for (bool m : mark)
+        if (!m) {
+            printf("parameter error!\n Please use -help to see the manual\n");
+            return -1;
+        }
+    if (std::fabs(A.threshold - 520) < 0.0001) {                       // ICONGPU.cu:317-323
+        if (A.data_type == 1) A.threshold = 0.03f;
+        if (A.data_type == 2) A.threshold = -0.03f;
+    }
+    int slicetotal = A.yend - A.ystart + 1;
+    printf("parameter:\ninput : %s\ntiltfile : %s\noutputPath : %s\nslice : %d,%d\n", A.input.c_str(), A.tilt.c_str(),
+           A.out.c_str(), A.ystart, A.yend);
+    printf("ICONIteration : %d,%d,%d\ndataType : %d\nthreshold : %f\n", A.iters[0], A.iters[1], A.iters[2], A.data_type,
+           A.threshold);
+    if (A.thickness != 0) printf("thickness : %d\n", A.thickness);
+    int used = std::min((int)A.gpus.size(), std::max(slicetotal, 0));
+    printf("use GPU : ");
+    for (int d = 0; d < used; ++d) printf("%d ", A.gpus[d]);
+    printf("\n");
+    if (used == 0) {
+        printf("Notice : No GPU is specified to use!\n");
+        return 0;
+    }
+    if (A.skip_cv == 1) printf("skip cross validation!\n");
+    std::string cvdir = join(A.out, "crossValidation"), recdir = join(A.out, "reconstruction");
+    mkdir(cvdir.c_str(), 0755);
+    mkdir(recdir.c_str(), 0755);
+
+    MrcHeader inh;
+    std::string err;
+    if (!mrc_read_header(A.input, inh, err)) {
+        printf("%s\n", err.c_str());
+        return 1;
+    }
+    std::vector<float> tilts;
+    {
+        FILE *tf = fopen(A.tilt.c_str(), "r");
+        if (!tf) {
+            printf("\nCan not open anglefile!\n");
+            return 1;
+        }
+        float t;
+        while (fscanf(tf, "%f", &t) == 1) tilts.push_back(t);
+        fclose(tf);
+    }
+    if ((int)tilts.size() != inh.nz) {
+        printf("tilt file has %zu angles but the stack has %d sections\n", tilts.size(), inh.nz);
+        return 1;
+    }
+    if (A.ystart < 0 || A.yend >= inh.ny || slicetotal <= 0) {
+        printf("slice range %d,%d outside 0..%d\n", A.ystart, A.yend, inh.ny - 1);
+        return 1;
+    }
+    const int thickness = A.thickness == 0 ? inh.nx : A.thickness;   // MainCode.cu:14-16
+    std::vector<float> stack;
+    if (!mrc_read_sections(A.input, inh, 0, inh.nz, stack, err)) {
+        printf("%s\n", err.c_str());
+        return 1;
+    }
+    // Tilt of the smallest |angle| among the negated angles (MainCode.cu:46-49).
+    int omit = 0;
+    {
+        float om = -tilts[0];
+        for (int k = 0; k < (int)tilts.size(); ++k)
+            if (std::fabs(om) > std::fabs(-tilts[k])) {
+                om = -tilts[k];
+                omit = k;
+            }
+    }
+    // Slice partition in proportion to SM count (ICONGPU.cu:398-449).
+    std::vector<Job> jobs(used);
+    {
+        double smsum = 0;
+        for (int d = 0; d < used; ++d) smsum += std::max(1, A.gpus[d] < (int)sm.size() ? sm[A.gpus[d]] : 1);
+        int start = 0;
+        for (int d = 0; d < used; ++d) {
+            int share = (d == used - 1) ? slicetotal - start
+                                        : (int)std::floor(std::max(1, sm[A.gpus[d]]) / smsum * slicetotal);
+            jobs[d].device = A.gpus[d];
+            jobs[d].y0 = A.ystart + start;
+            jobs[d].y1 = A.ystart + start + share;
+            printf("thread %d using GPU %d , deals with slices : start %d end %d\n", d, A.gpus[d], jobs[d].y0, jobs[d].y1 - 1);
+            start += share;
+        }
+    }
+    std::vector<float> rp_full((size_t)slicetotal * inh.nx, 0.f), rp_cv((size_t)slicetotal * inh.nx, 0.f);
+    std::vector<float> volume;
+    if (!A.volume.empty()) volume.assign((size_t)slicetotal * inh.nx * thickness, 0.f);
+    std::vector<std::thread> threads;
+    for (auto &job : jobs)
+        threads.emplace_back([&, jp = &job] {
+            run_job(*jp, A, inh, tilts, thickness, stack, omit, rp_full, rp_cv, volume.empty() ? nullptr : &volume, recdir);
+        });
+    for (auto &t : threads) t.join();
+    for (auto &job : jobs)
+        if (job.rc) {
+            printf("running state: fail!\nError message: %s\n", job.err.c_str());
+            return 1;
+        }
+    if (!A.volume.empty()) {
+        MrcHeader vh = inh;
+        vh.nx = inh.nx;
+        vh.ny = thickness;
+        vh.nz = slicetotal;
+        vh.mx = inh.nx;
+        vh.my = thickness;
+        vh.mz = slicetotal;
+        vh.next = 0;
+        if (!mrc_write_float(A.volume, vh, volume.data(), err)) {
+            printf("%s\n", err.c_str());
+            return 1;
+        }
+    }
+    if (A.skip_cv == 0) {                                               // ICONGPU.cu:468-592
+        std::vector<float> gt((size_t)slicetotal * inh.nx);
+        for (int y = A.ystart, k = 0; y <= A.yend; ++y, ++k)
+            std::memcpy(&gt[(size_t)k * inh.nx], &stack[((size_t)omit * inh.ny + y) * inh.nx], sizeof(float) * inh.nx);
+        auto save2d = [&](const std::string &name, const std::vector<float> &d) {
+            MrcHeader oh = inh;                                          // saveMRC_real.cu:9-31
+            oh.mz = inh.mx;
+            oh.zlen = inh.xlen;
+            oh.nx = inh.nx;
+            oh.ny = slicetotal;
+            oh.nz = 1;
+            std::string e;
+            if (!mrc_write_float(join(cvdir, name), oh, d.data(), e)) printf("%s\n", e.c_str());
+        };
+        save2d("GroundTruth.mrc", gt);
+        save2d("fullRec_reProjection.mrc", rp_full);
+        save2d("crossV_reprojection.mrc", rp_cv);
+        int half = inh.nx / 2;
+        double resstep = 1.0 / inh.nx;
+        auto write_frc = [&](const std::string &name, const std::vector<float> &rp) {
+            std::vector<float> frc = frc_nonsquare(gt, rp, inh.nx, slicetotal);
+            frc_smooth(frc, half, 10);
+            FILE *f = fopen(join(cvdir, name).c_str(), "w");
+            if (!f) return;
+            for (int k = 0; k < half; ++k) fprintf(f, "%f %f\n", resstep * k, frc[k]);
+            fclose(f);
+        };
+        write_frc("fullRec.frc", rp_full);
+        write_frc("crossV.frc", rp_cv);
+    }
+    printf("running state:\n   ICON-GPU finish!\n");
+    return 0;
+}

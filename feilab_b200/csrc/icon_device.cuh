@@ -120,6 +120,256 @@ __device__ __forceinline__ void fft_smem(float2 *s, int n, int lg, int B, const 
     }
 }
 
+// ---- batched FFT with compile-time batch B and row stride SB (>= B) ----
+// Same Stockham passes as fft_pass/fft_smem over s[n][SB] (values of slice b
+// at s[pos*SB + b]); B and SB are powers of two or padded strides known at
+// compile time, so all index arithmetic is shifts and masks.
+template <int B>
+struct Log2B {
+    static constexpr int v = (B >= 8) ? 3 : (B >= 4) ? 2 : (B >= 2) ? 1 : 0;
+};
+
+template <int R, int B, int SB>
+__device__ __forceinline__ void fft_pass_b(float2 *s, int n, int Ns, const float2 *__restrict__ tw, float dir)
+{
+    constexpr int Q = 16 / R;
+    constexpr int LB = Log2B<B>::v;
+    const int nb = n / R;
+    const int T = blockDim.x;
+    const int step = n / (Ns * R);
+    float2 v[Q][R];
+    int jq[Q], bq[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        int item = threadIdx.x + q * T;
+        int b = item & (B - 1), j = item >> LB;
+        jq[q] = j;
+        bq[q] = b;
+        int k = j & (Ns - 1);
+        float2 in[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) in[r] = s[(j + r * nb) * SB + b];
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                float2 w = __ldg(&tw[r * k * step]);
+                w.y = -dir * w.y;
+                in[r] = cmul(in[r], w);
+            }
+        }
+        dft<R, 1>(in, v[q], dir);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        int j = jq[q], b = bq[q];
+        int k = j & (Ns - 1);
+        int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) s[(base + r * Ns) * SB + b] = v[q][r];
+    }
+    __syncthreads();
+}
+
+// blockDim.x == n*B/16; call after a __syncthreads().
+template <int B, int SB>
+__device__ __forceinline__ void fft_batched(float2 *s, int n, int lg, const float2 *__restrict__ tw, float dir)
+{
+    int Ns = 1;
+    switch (lg & 3) {
+    case 1: fft_pass_b<2, B, SB>(s, n, Ns, tw, dir); Ns = 2; break;
+    case 2: fft_pass_b<4, B, SB>(s, n, Ns, tw, dir); Ns = 4; break;
+    case 3: fft_pass_b<8, B, SB>(s, n, Ns, tw, dir); Ns = 8; break;
+    default: break;
+    }
+    while (Ns < n) {
+        fft_pass_b<16, B, SB>(s, n, Ns, tw, dir);
+        Ns *= 16;
+    }
+}
+
+// ---- fused FFT: E values per thread, I/O through functors ---------------
+// exp(dir * 2*pi*i * k / 32) for compile-time k.
+__device__ __forceinline__ float2 w32(int k, float dir)
+{
+    constexpr float C[32] = {
+        1.0f, 0.98078528040323043f, 0.92387953251128674f, 0.83146961230254524f, 0.70710678118654752f,
+        0.55557023301960218f, 0.38268343236508977f, 0.19509032201612826f, 0.0f, -0.19509032201612826f,
+        -0.38268343236508977f, -0.55557023301960218f, -0.70710678118654752f, -0.83146961230254524f,
+        -0.92387953251128674f, -0.98078528040323043f, -1.0f, -0.98078528040323043f, -0.92387953251128674f,
+        -0.83146961230254524f, -0.70710678118654752f, -0.55557023301960218f, -0.38268343236508977f,
+        -0.19509032201612826f, 0.0f, 0.19509032201612826f, 0.38268343236508977f, 0.55557023301960218f,
+        0.70710678118654752f, 0.83146961230254524f, 0.92387953251128674f, 0.98078528040323043f};
+    return make_float2(C[k & 31], dir * C[(k + 24) & 31]);
+}
+
+// out[q] = sum_r in[r*IS] exp(dir*2*pi*i*r*q/R), R <= 32, unrolled.
+template <int R, int IS>
+__device__ __forceinline__ void dft32(const float2 *in, float2 *out, float dir)
+{
+    if constexpr (R == 1) {
+        out[0] = in[0];
+    } else {
+        float2 e[R / 2], o[R / 2];
+        dft32<R / 2, 2 * IS>(in, e, dir);
+        dft32<R / 2, 2 * IS>(in + IS, o, dir);
+#pragma unroll
+        for (int k = 0; k < R / 2; ++k) {
+            float2 t = (k == 0) ? o[k] : cmul(w32(k * (32 / R), dir), o[k]);
+            out[k] = cadd(e[k], t);
+            out[k + R / 2] = csub(e[k], t);
+        }
+    }
+}
+
+// Bit reversal of r < 32 over 5 bits, branch- and loop-free so that it folds
+// to a constant for unrolled r.
+__host__ __device__ constexpr int brev5(int r)
+{
+    return ((r & 1) << 4) | ((r & 2) << 2) | (r & 4) | ((r & 8) >> 2) | ((r & 16) >> 4);
+}
+
+template <int R>
+struct Lg {
+    static constexpr int v = R >= 32 ? 5 : R >= 16 ? 4 : R >= 8 ? 3 : R >= 4 ? 2 : R >= 2 ? 1 : 0;
+};
+
+// One radix-2 stage (butterfly span LEN) of the in-place DIT DFT below, then
+// the next stage; template recursion keeps every index a compile-time constant.
+template <int R, int LEN>
+__device__ __forceinline__ void dft_stage(float2 (&a)[R], float dir)
+{
+#pragma unroll
+    for (int i = 0; i < R; i += LEN) {
+#pragma unroll
+        for (int k = 0; k < LEN / 2; ++k) {
+            float2 o = a[i + k + LEN / 2];
+            float2 t = (k == 0) ? o : cmul(w32((k * (32 / LEN)) & 31, dir), o);
+            a[i + k + LEN / 2] = csub(a[i + k], t);
+            a[i + k] = cadd(a[i + k], t);
+        }
+    }
+    if constexpr (LEN < R) dft_stage<R, 2 * LEN>(a, dir);
+}
+
+// In-place radix-2 DIT DFT of R values held in registers, a[] given in
+// bit-reversed order; on return a[q] = sum_r x[r] exp(dir*2*pi*i*r*q/R).
+// Only the R values are live, so a 32-point DFT needs 64 registers.
+template <int R>
+__device__ __forceinline__ void dft_inplace(float2 (&a)[R], float dir)
+{
+    if constexpr (R >= 2) dft_stage<R, 2>(a, dir);
+}
+
+// One Stockham pass of radix R over n points for B slices, E values per
+// thread (E/R butterflies).  FIRST: inputs come from ld(pos, b) instead of
+// s[pos*SB + b]; LAST: outputs go to st(pos, b, value) instead of s.  A
+// barrier separates the reads of a pass from its writes, so ld may read s
+// and st may write s; the caller syncs after a LAST pass if st wrote s.
+template <int R, int B, int SB, int E, bool FIRST, bool LAST, bool GUARD, class Ld, class St>
+__device__ __forceinline__ void fpass(float2 *s, int n, int Ns, const float2 *__restrict__ tw, float dir, Ld &ld, St &st,
+                                      int T)
+{
+    constexpr int Q = E / R;
+    constexpr int LB = Log2B<B>::v;
+    const int nb = n / R;
+    const bool act = !GUARD || (int)threadIdx.x < T;
+    const int step = n / (Ns * R);
+    float2 v[Q][R];
+    if (act) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            int item = threadIdx.x + q * T;
+            int b = item & (B - 1), j = item >> LB;
+            int k = j & (Ns - 1);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                float2 x;
+                if constexpr (FIRST) x = ld(j + r * nb, b);
+                else x = s[(j + r * nb) * SB + b];
+                if (!FIRST && r > 0 && Ns > 1) {
+                    float2 w = __ldg(&tw[r * k * step]);
+                    w.y = -dir * w.y;
+                    x = cmul(x, w);
+                }
+                v[q][brev5(r) >> (5 - Lg<R>::v)] = x;
+            }
+            dft_inplace<R>(v[q], dir);
+        }
+    }
+    __syncthreads();   // all reads of s (or of ld's buffer) done before any write
+    if (act) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            int item = threadIdx.x + q * T;
+            int b = item & (B - 1), j = item >> LB;
+            int k = j & (Ns - 1);
+            int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if constexpr (LAST) st(base + r * Ns, b, v[q][r]);
+                else s[(base + r * Ns) * SB + b] = v[q][r];
+            }
+        }
+    }
+    if constexpr (!LAST) __syncthreads();
+}
+
+template <int R, int B, int SB, int E, bool GUARD, class Ld, class St>
+__device__ __forceinline__ void fpass_any(bool first, bool last, float2 *s, int n, int Ns, const float2 *tw, float dir,
+                                          Ld &ld, St &st, int T)
+{
+    if (first) {
+        if (last) fpass<R, B, SB, E, true, true, GUARD>(s, n, Ns, tw, dir, ld, st, T);
+        else fpass<R, B, SB, E, true, false, GUARD>(s, n, Ns, tw, dir, ld, st, T);
+    } else {
+        if (last) fpass<R, B, SB, E, false, true, GUARD>(s, n, Ns, tw, dir, ld, st, T);
+        else fpass<R, B, SB, E, false, false, GUARD>(s, n, Ns, tw, dir, ld, st, T);
+    }
+}
+
+// Unnormalised FFT of length n = 2^lg for each of B slices, computed by the
+// first n*B/E threads of the block: blockDim.x == n*B/E unless GUARD, in which
+// case extra threads only take part in the barriers.  The first pass reads ld(pos, b) (natural order), the last pass
+// hands st(pos, b, value) the outputs in natural order; intermediate passes
+// use s[n][SB].  The first pass has no twiddles (Ns = 1).  E is 16 or 32:
+// passes of radix E after one pass of radix 2^(lg mod log2 E).
+template <int B, int SB, int E, bool GUARD = false, class Ld, class St>
+__device__ __forceinline__ void fft_fused(float2 *s, int n, int lg, const float2 *__restrict__ tw, float dir, Ld &ld, St &st)
+{
+    constexpr int LE = (E == 32) ? 5 : 4;
+    const int T = n * B / E;
+    const int rem = lg % LE;
+    int Ns = 1;
+    bool first = true;
+    if (rem) {
+        bool last = (1 << rem) == n;
+        switch (rem) {
+        case 1: fpass_any<2, B, SB, E, GUARD>(first, last, s, n, Ns, tw, dir, ld, st, T); break;
+        case 2: fpass_any<4, B, SB, E, GUARD>(first, last, s, n, Ns, tw, dir, ld, st, T); break;
+        case 3: fpass_any<8, B, SB, E, GUARD>(first, last, s, n, Ns, tw, dir, ld, st, T); break;
+        default:
+            if constexpr (E == 32) fpass_any<16, B, SB, E, GUARD>(first, last, s, n, Ns, tw, dir, ld, st, T);
+            break;
+        }
+        Ns = 1 << rem;
+        first = false;
+    }
+    while (Ns < n) {
+        bool last = Ns * E == n;
+        fpass_any<E, B, SB, E, GUARD>(first, last, s, n, Ns, tw, dir, ld, st, T);
+        Ns *= E;
+        first = false;
+    }
+}
+
+// Row stride (in float2) of the gather buffers: padded so that 16-byte loads
+// of eight neighbouring rows fall in different banks.
+template <int B>
+struct RowStride {
+    static constexpr int v = (B == 8) ? 10 : (B == 4) ? 6 : B;
+};
+
 // Deterministic block reduction of per-thread doubles where thread t holds a
 // value for slice t % B; blockDim.x is a multiple of B and a power of two.
 // Returns, in threads t < B, the sum for slice t.  scratch: blockDim.x doubles.

@@ -1,0 +1,126 @@
+// icon_kern_b.cu -- the batched FFT kernels for one slice-group size,
+// ICON_KB (1, 2, 4 or 8, set by the build), and their host launchers.
+#define ICON_KERNELS_TEMPLATES_ONLY
+#include "icon_kernels.cuh"
+#include "icon_launch.h"
+
+#ifndef ICON_KB
+#error "compile with -DICON_KB=<1|2|4|8>"
+#endif
+
+namespace icon {
+
+template <int B>
+void Launch<B>::xpass_fwd(bool real_in, int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
+                          const void *in, float2 *G1)
+{
+    if (E == 32) {
+        if (real_in) k_xpass_fwd<true, B, 32><<<grid, threads, smem, st>>>(g, in, G1);
+        else k_xpass_fwd<false, B, 32><<<grid, threads, smem, st>>>(g, in, G1);
+    } else {
+        if (real_in) k_xpass_fwd<true, B, 16><<<grid, threads, smem, st>>>(g, in, G1);
+        else k_xpass_fwd<false, B, 16><<<grid, threads, smem, st>>>(g, in, G1);
+    }
+}
+
+template <int B>
+void Launch<B>::ypass_fwd(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const float2 *G1,
+                          float2 *P)
+{
+    if (E == 32) k_ypass_fwd<B, 32><<<grid, threads, smem, st>>>(g, G1, P);
+    else k_ypass_fwd<B, 16><<<grid, threads, smem, st>>>(g, G1, P);
+}
+
+template <int B>
+void Launch<B>::interp_fin(int mode, dim3 grid, cudaStream_t st, const Geo &g, const float2 *P, float2 *f, double *part)
+{
+    if (mode == 0) k_interp_fin<0, B><<<grid, 256, 0, st>>>(g, P, f, part);
+    else if (mode == 1) k_interp_fin<1, B><<<grid, 256, 0, st>>>(g, P, f, part);
+    else k_interp_fin<2, B><<<grid, 256, 0, st>>>(g, P, f, part);
+}
+
+template <int B>
+void Launch<B>::ypass_adj(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const float2 *f,
+                          float2 *G1)
+{
+    // The band loop needs a full warp; tiny FFTs have fewer threads than that.
+    bool guard = threads < 32;
+    if (guard) threads = 32;
+    if (E == 32) k_ypass_adj<B, 32, false><<<grid, threads, smem, st>>>(g, f, G1);
+    else if (!guard) k_ypass_adj<B, 16, false><<<grid, threads, smem, st>>>(g, f, G1);
+    else k_ypass_adj<B, 16, true><<<grid, threads, smem, st>>>(g, f, G1);
+}
+
+template <int B>
+void Launch<B>::xpass_adj(int mode, int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
+                          const float2 *G1, float2 *out, const float2 *Ahwb, double *part)
+{
+    if (E == 32) {
+        if (mode == 0) k_xpass_adj<0, B, 32><<<grid, threads, smem, st>>>(g, G1, out, Ahwb, part);
+        else k_xpass_adj<1, B, 32><<<grid, threads, smem, st>>>(g, G1, out, Ahwb, part);
+    } else {
+        if (mode == 0) k_xpass_adj<0, B, 16><<<grid, threads, smem, st>>>(g, G1, out, Ahwb, part);
+        else k_xpass_adj<1, B, 16><<<grid, threads, smem, st>>>(g, G1, out, Ahwb, part);
+    }
+}
+
+template <int B>
+void Launch<B>::rows_fwd(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const Geo1 &g1,
+                         const float *rows, int S, float2 *f, float2 *bout)
+{
+    if (E == 32) k_rows_fwd<B, 32><<<grid, threads, smem, st>>>(g, g1, rows, S, f, bout);
+    else k_rows_fwd<B, 16><<<grid, threads, smem, st>>>(g, g1, rows, S, f, bout);
+}
+
+template <int B>
+void Launch<B>::row_adj(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const Geo1 &g1,
+                        const float2 *f, float *out, int S)
+{
+    if (E == 32) k_row_adj<B, 32><<<grid, threads, smem, st>>>(g, g1, f, out, S);
+    else k_row_adj<B, 16><<<grid, threads, smem, st>>>(g, g1, f, out, S);
+}
+
+template <int B>
+void Launch<B>::update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat, const double *alpha, int per_group,
+                       int clamp, int data_type, float thr)
+{
+    k_update<B><<<grid, 256, 0, st>>>(m, rhat, alpha, per_group, clamp, data_type, thr);
+}
+
+template <int B>
+cudaError_t Launch<B>::set_smem(int ex, int ey, size_t smem_x, size_t need_x, size_t smem_y, size_t smem_ya)
+{
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void *fn, size_t bytes) {
+        cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (r != cudaSuccess && e == cudaSuccess) e = r;
+    };
+    if (ex == 32) {
+        set((const void *)k_xpass_fwd<true, B, 32>, smem_x);
+        set((const void *)k_xpass_fwd<false, B, 32>, smem_x);
+        set((const void *)k_xpass_adj<0, B, 32>, need_x);
+        set((const void *)k_xpass_adj<1, B, 32>, need_x);
+        set((const void *)k_rows_fwd<B, 32>, smem_x);
+        set((const void *)k_row_adj<B, 32>, smem_x);
+    } else {
+        set((const void *)k_xpass_fwd<true, B, 16>, smem_x);
+        set((const void *)k_xpass_fwd<false, B, 16>, smem_x);
+        set((const void *)k_xpass_adj<0, B, 16>, need_x);
+        set((const void *)k_xpass_adj<1, B, 16>, need_x);
+        set((const void *)k_rows_fwd<B, 16>, smem_x);
+        set((const void *)k_row_adj<B, 16>, smem_x);
+    }
+    if (ey == 32) {
+        set((const void *)k_ypass_fwd<B, 32>, smem_y);
+        set((const void *)k_ypass_adj<B, 32, false>, smem_ya);
+    } else {
+        set((const void *)k_ypass_fwd<B, 16>, smem_y);
+        set((const void *)k_ypass_adj<B, 16, false>, smem_ya);
+        set((const void *)k_ypass_adj<B, 16, true>, smem_ya);
+    }
+    return e;
+}
+
+template struct Launch<ICON_KB>;
+
+}  // namespace icon

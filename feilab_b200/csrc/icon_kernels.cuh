@@ -3,7 +3,7 @@
 // The reference (ICON-GPU v1.2.9, NU = nufft_gpu_v8.cu) computes a NUFFT as
 // pre-pass -> full 2-D cuFFT of the n0 x n1 grid -> interpolation (forward), or
 // CSR gather onto the grid -> 2-D cuFFT -> crop (adjoint), one slice at a time.
-// Here a batch of B slices moves through two FFT passes whose far ends are
+// Here a group of B slices moves through two FFT passes whose far ends are
 // fused with the non-uniform step, so the oversampled grid is never stored:
 //
 //   forward   K1  xpass_fwd   per (column Y, group): deapodise + pad + shift
@@ -15,31 +15,44 @@
 //                             the y-interpolation sum_t1 phiy*G -> P[j][t0][b]
 //             K3  interp_fin  per node: f_j = sum_t0 phix * P[j][t0]
 //                             (+ weighting / step-length partial sums)
-//   adjoint   K2T ypass_adj   per (row x, group): gather every node's
-//                             contribution on row x into shared memory (no
+//   adjoint   K2T ypass_adj   per (row x, group): every buffer row gathers
+//                             the window entries covering it (sorted, no
 //                             atomics), inverse FFT along y, keep the N1 rows
 //                             the crop keeps -> G1[x][Y][b]
 //             K1T xpass_adj   per (column Y, group): inverse FFT along x,
 //                             crop, divide by the deapodisation
 //                             (+ r = fhat - Ahwb and ||r||^2 partial sums)
+//
+// Rows of the y-pass are held in shared memory rotated by n1/2, so that the
+// unwrapped tap position u = iy0 + t1 in [-n1/2-6, n1/2+6] is row u + n1/2 of
+// the buffer, with 8 halo rows on each side (copies of the other end); no tap
+// needs a modulo.  The rotation costs nothing: multiplying the FFT input by
+// (-1)^y shifts its output by n1/2, and an input rotated by n1/2 gives the
+// output times (-1)^k.
 #pragma once
 #include "icon_device.cuh"
 
 namespace icon {
+
+constexpr int kHalo = 8;      // halo rows on each side of a rotated row buffer
+constexpr int kLdPhiy = 16;   // phiy rows padded to 16 floats (four 16-byte loads)
 
 // Device view of one tilt-series geometry (all pointers are device memory).
 struct Geo {
     int N0, N1, n0, n1, lg0, lg1, M, nx, nz, B;
     const float *w;        // [M] density weights (Weight, weight.cu:8-41)
     const float *phix;     // [M][14] window values, x taps   (NU:221-235)
-    const float *phiy;     // [M][14] window values, y taps
+    const float *phiy;     // [M][16] window values, y taps, 2 zero pads
     const int *ix0;        // [M] first x tap, unwrapped: floor(n0*x0) - 6
     const int *iy0;        // [M] first y tap, unwrapped
     const float *cx;       // [N0] deapodisation factor along x (NU:22-42)
     const float *cy;       // [N1] deapodisation factor along y
+    const float *rcx;      // [N0] 1/cx, rounded once from double
+    const float *rcy;      // [N1] 1/cy
     const int *row_off;    // [n0+1] entry range of every grid row x
     const int *ent_jt;     // [M*14] entry: node*16 + x tap, sorted by (row, iy0, node)
     const int *ent_iy0;    // [M*14] iy0 of the entry's node (sort key within a row)
+    const unsigned short *ent_lb;   // [n0][n1+17] per-row lower bounds of r0 (k_ypass_adj)
     const float2 *tw0;     // [n0] exp(-2 pi i q / n0)
     const float2 *tw1;     // [n1] exp(-2 pi i q / n1)
 };
@@ -50,11 +63,13 @@ struct Geo1 {
     const int *i10;        // [nx] first tap, unwrapped, nondecreasing in k
 };
 
+#ifndef ICON_KERNELS_TEMPLATES_ONLY
 // ------------------------------------------------------------- tables ----
 // Window taps exactly as nufft_Phi2d_1dCU (NU:221-235) computes them, in float:
-// l = floor(n*x) - m + t, x1 = x - l/n, phi = bf*exp(-(n*x1)^2/b).
+// l = floor(n*x) - m + t, x1 = x - l/n, phi = bf*exp(-(n*x1)^2/b).  Rows of
+// ld >= 14 floats, the pad zeroed.
 __global__ void k_window(const float *__restrict__ x, int stride, int M, int n, float b, float bf,
-                         float *__restrict__ phi, int *__restrict__ l0out)
+                         float *__restrict__ phi, int ld, int *__restrict__ l0out)
 {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= M) return;
@@ -65,43 +80,94 @@ __global__ void k_window(const float *__restrict__ x, int stride, int M, int n, 
     for (int t = 0; t < kTaps; ++t) {
         int l = l0 + t;
         float x1 = xv - (float)l / (float)n;
-        phi[(size_t)j * kTaps + t] = bf * expf(-((n * x1) * (n * x1) / b));
+        phi[(size_t)j * ld + t] = bf * expf(-((n * x1) * (n * x1) / b));
+    }
+    for (int t = kTaps; t < ld; ++t) phi[(size_t)j * ld + t] = 0.f;
+}
+
+#endif  // ICON_KERNELS_TEMPLATES_ONLY
+
+// Loads B consecutive float2 (16-byte vector loads when B is even).
+template <int B>
+__device__ __forceinline__ void load_b(const float2 *__restrict__ p, float2 (&v)[B])
+{
+    if constexpr (B % 2 == 0) {
+#pragma unroll
+        for (int i = 0; i < B / 2; ++i) {
+            float4 t = reinterpret_cast<const float4 *>(p)[i];
+            v[2 * i] = make_float2(t.x, t.y);
+            v[2 * i + 1] = make_float2(t.z, t.w);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < B; ++i) v[i] = p[i];
     }
 }
+
+template <int B>
+__device__ __forceinline__ void store_b(float2 *__restrict__ p, const float2 (&v)[B])
+{
+    if constexpr (B % 2 == 0) {
+#pragma unroll
+        for (int i = 0; i < B / 2; ++i)
+            reinterpret_cast<float4 *>(p)[i] = make_float4(v[2 * i].x, v[2 * i].y, v[2 * i + 1].x, v[2 * i + 1].y);
+    } else {
+#pragma unroll
+        for (int i = 0; i < B; ++i) p[i] = v[i];
+    }
+}
+
+// Launch bound of the FFT kernels: blockDim = n*B/E <= 512 threads for E = 32
+// (so up to 128 registers), <= 1024 for E = 16.
+#define FFT_BOUNDS(E) __launch_bounds__((E) == 32 ? 512 : 1024)
 
 // --------------------------------------------------------------- K1 ----
 // Forward x-pass.  in: [G][N1][N0][B] real (m) or complex; out G1 [G][n0][N1][B].
 // Pre-pass of NU:784-809 / NU:754-781: grid x holds img[X]/ck(X,Y) with
-// X = (x + N0/2) % n0 when X < N0, else 0; ck = cx[X]*cy[Y] in float.
-template <bool REAL_IN>
-__global__ void __launch_bounds__(1024) k_xpass_fwd(Geo g, const void *__restrict__ in, float2 *__restrict__ G1)
+// X = (x + N0/2) % n0 when X < N0, else 0; ck = cx[X]*cy[Y] (the division is
+// a multiplication by the reciprocals, within 2 ulp of the reference's
+// quotient).  The first FFT pass reads the image column directly, the last
+// writes G1.
+template <bool REAL_IN, int B, int E>
+__global__ void FFT_BOUNDS(E) k_xpass_fwd(Geo g, const void *__restrict__ in, float2 *__restrict__ G1)
 {
     extern __shared__ float2 s[];
-    const int Y = blockIdx.x, grp = blockIdx.y, B = g.B, n = g.n0, N0 = g.N0;
-    const float cyY = g.cy[Y];
-    const size_t ibase = ((size_t)grp * g.N1 + Y) * N0 * B;
-    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
-        int b = idx % B, x = idx / B;
-        int X = (x + N0 / 2) % n;
-        float2 v = make_float2(0.f, 0.f);
-        if (X < N0) {
-            float ck = g.cx[X] * cyY;
-            if (REAL_IN) {
-                v.x = ((const float *)in)[ibase + (size_t)X * B + b] / ck;
-            } else {
-                float2 t = ((const float2 *)in)[ibase + (size_t)X * B + b];
-                v.x = t.x / ck;
-                v.y = t.y / ck;
-            }
+    const int Y = blockIdx.x, grp = blockIdx.y, n = g.n0, N0 = g.N0, N1 = g.N1;
+    const float rcyY = g.rcy[Y];
+    const float *rcx = g.rcx;
+    const size_t ibase = ((size_t)grp * N1 + Y) * N0 * B;
+    float2 *out = G1 + (size_t)grp * n * N1 * B + (size_t)Y * B;
+    // Stage the deapodised column [N0][B] (contiguous in global memory); the
+    // first FFT pass reads it before anything is written to s.
+    for (int idx = threadIdx.x; idx < N0 * B; idx += blockDim.x) {
+        float r = rcx[idx / B] * rcyY;
+        float2 v;
+        if (REAL_IN) v = make_float2(((const float *)in)[ibase + idx] * r, 0.f);
+        else {
+            float2 t = ((const float2 *)in)[ibase + idx];
+            v = make_float2(t.x * r, t.y * r);
         }
         s[idx] = v;
     }
     __syncthreads();
-    fft_smem(s, n, g.lg0, B, g.tw0, -1.f);
-    const size_t obase = (size_t)grp * n * g.N1 * B;
-    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
-        int b = idx % B, x = idx / B;
-        G1[obase + ((size_t)x * g.N1 + Y) * B + b] = s[idx];
+    auto ld = [=](int x, int b) -> float2 {
+        int X = (x + N0 / 2) & (n - 1);
+        return (X < N0) ? s[X * B + b] : make_float2(0.f, 0.f);
+    };
+    auto st = [=](int x, int b, float2 v) { out[(size_t)x * N1 * B + b] = v; };
+    fft_fused<B, B, E>(s, n, g.lg0, g.tw0, -1.f, ld, st);
+}
+
+// Copies the wrap-around halo rows of a rotated row buffer (rows 0..7 and
+// n+8..n+15 of s[(n + 16)][SB]).
+template <int B, int SB>
+__device__ __forceinline__ void fill_halo(float2 *s, int n)
+{
+    constexpr int LB = Log2B<B>::v;
+    for (int idx = threadIdx.x; idx < kHalo * B; idx += blockDim.x) {
+        int b = idx & (B - 1), i = idx >> LB;
+        s[i * SB + b] = s[(i + n) * SB + b];
+        s[(n + kHalo + i) * SB + b] = s[(kHalo + i) * SB + b];
     }
 }
 
@@ -110,38 +176,60 @@ __global__ void __launch_bounds__(1024) k_xpass_fwd(Geo g, const void *__restric
 // the N1 nonzero columns; column Y sits at y with (y + N1/2) % n1 == Y.
 // P[G][M][14][B]: P[j][t0] = sum_t1 phiy[j][t1] * G[x][(iy0_j + t1) mod n1],
 // x = (ix0_j + t0) mod n0.  (NU:669-727 sum the same 196 products per node.)
-__global__ void __launch_bounds__(1024) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, float2 *__restrict__ P)
+// The first FFT pass reads G1 directly; one thread per entry computes all B
+// slices of it from the rotated row in shared memory.
+template <int B, int E>
+__global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, float2 *__restrict__ P)
 {
     extern __shared__ float2 s[];
-    const int x = blockIdx.x, grp = blockIdx.y, B = g.B, n = g.n1, N1 = g.N1;
-    const size_t rbase = ((size_t)grp * g.n0 + x) * N1 * B;
-    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
-        int b = idx % B, y = idx / B;
-        int Y = (y + N1 / 2) % n;
-        s[idx] = (Y < N1) ? G1[rbase + (size_t)Y * B + b] : make_float2(0.f, 0.f);
-    }
+    constexpr int SB = RowStride<B>::v;
+    const int x = blockIdx.x, grp = blockIdx.y, n = g.n1, N1 = g.N1;
+    const float2 *rowin = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
+    float2 *row = s + kHalo * SB;
+    // Stage the N1 nonzero values of the row (contiguous in G1).
+    for (int idx = threadIdx.x; idx < N1 * B; idx += blockDim.x) row[idx] = rowin[idx];
     __syncthreads();
-    fft_smem(s, n, g.lg1, B, g.tw1, -1.f);
-    const int e0 = g.row_off[x], ne = g.row_off[x + 1] - e0;
+    auto ld = [=](int y, int b) -> float2 {
+        int Y = (y + N1 / 2) & (n - 1);
+        float2 v = (Y < N1) ? row[Y * B + b] : make_float2(0.f, 0.f);
+        return (y & 1) ? make_float2(-v.x, -v.y) : v;      // rotates the output by n/2
+    };
+    auto st = [=](int q, int b, float2 v) { row[q * SB + b] = v; };
+    fft_fused<B, SB, E>(row, n, g.lg1, g.tw1, -1.f, ld, st);
+    __syncthreads();
+    fill_halo<B, SB>(s, n);
+    __syncthreads();
+    const int e0 = g.row_off[x], e1 = g.row_off[x + 1];
     const size_t pbase = (size_t)grp * g.M * kTaps * B;
-    for (int idx = threadIdx.x; idx < ne * B; idx += blockDim.x) {
-        int b = idx % B, e = e0 + idx / B;
+    const int rofs = n / 2 + kHalo;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
         int jt = __ldg(&g.ent_jt[e]);
         int j = jt >> 4, t0 = jt & 15;
-        int iy = __ldg(&g.ent_iy0[e]);
-        const float *py = g.phiy + (size_t)j * kTaps;
-        float2 acc = make_float2(0.f, 0.f);
+        const float2 *sr = s + (__ldg(&g.ent_iy0[e]) + rofs) * SB;
+        const float4 *py4 = reinterpret_cast<const float4 *>(g.phiy + (size_t)j * kLdPhiy);
+        float py[16];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float4 t = __ldg(&py4[i]);
+            py[4 * i] = t.x;
+            py[4 * i + 1] = t.y;
+            py[4 * i + 2] = t.z;
+            py[4 * i + 3] = t.w;
+        }
+        float2 acc[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) acc[b] = make_float2(0.f, 0.f);
 #pragma unroll
         for (int t1 = 0; t1 < kTaps; ++t1) {
-            int y = iy + t1;
-            y += (y < 0) ? n : 0;
-            y -= (y >= n) ? n : 0;
-            float2 v = s[y * B + b];
-            float p = __ldg(&py[t1]);
-            acc.x = fmaf(v.x, p, acc.x);
-            acc.y = fmaf(v.y, p, acc.y);
+            float2 v[B];
+            load_b<B>(sr + t1 * SB, v);
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                acc[b].x = fmaf(v[b].x, py[t1], acc[b].x);
+                acc[b].y = fmaf(v[b].y, py[t1], acc[b].y);
+            }
         }
-        P[pbase + ((size_t)j * kTaps + t0) * B + b] = acc;
+        store_b<B>(P + pbase + ((size_t)j * kTaps + t0) * B, acc);
     }
 }
 
@@ -150,13 +238,14 @@ __global__ void __launch_bounds__(1024) k_ypass_fwd(Geo g, const float2 *__restr
 // f*w (complexMulDoubleCU, NU:1539-1549).  MODE 2: store nothing; per-slice
 // partial sums of w*|f|^2 in double (alpha1, NU:1652-1661) into
 // part[G][gridDim.x][B].
-template <int MODE>
+template <int MODE, int B>
 __global__ void k_interp_fin(Geo g, const float2 *__restrict__ P, float2 *__restrict__ f, double *__restrict__ part)
 {
     __shared__ double red[256];
-    const int grp = blockIdx.y, B = g.B;
+    constexpr int LB = Log2B<B>::v;
+    const int grp = blockIdx.y;
     const int item = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = item / B, b = item % B;
+    const int j = item >> LB, b = item & (B - 1);
     double acc2 = 0.0;
     if (j < g.M) {
         const float *px = g.phix + (size_t)j * kTaps;
@@ -196,100 +285,189 @@ __device__ __forceinline__ int lower_bound_i(const int *__restrict__ key, int lo
     return lo;
 }
 
-// -------------------------------------------------------------- K2T ----
-// Adjoint y-pass.  Each grid point (x, y) of the row gathers, in a fixed order,
-// the contributions phix*phiy*f_j of the entries whose y footprint
-// [iy0, iy0+13] covers y (or y - n1: the footprint is unwrapped); the
-// reference gathers the same sums through its host-built CSR (NU:1078-1102).
-// Then the inverse FFT along y (NU:1203), and the rows Y < N1 of the crop
-// (NU:1104-1121: y = (Y + n1 - N1/2) % n1) go to G1[x][Y][b].
-__global__ void __launch_bounds__(1024) k_ypass_adj(Geo g, const float2 *__restrict__ f, float2 *__restrict__ G1)
+// Index of the first of the sorted keys key[lo..hi) that is >= v (shared memory).
+__device__ __forceinline__ int lower_bound_s(const int *key, int lo, int hi, int v)
 {
-    extern __shared__ float2 s[];
-    const int x = blockIdx.x, grp = blockIdx.y, B = g.B, n = g.n1, N1 = g.N1;
-    const int e0 = g.row_off[x], e1 = g.row_off[x + 1];
-    const float2 *fg = f + (size_t)grp * g.M * B;
-    for (int y = threadIdx.x; y < n; y += blockDim.x) {
-        float2 acc[8];
-#pragma unroll
-        for (int b = 0; b < 8; ++b) acc[b] = make_float2(0.f, 0.f);
-        // Unwrapped positions u of this y: y itself and y - n1.
-#pragma unroll
-        for (int al = 0; al < 2; ++al) {
-            int u = y - al * n;
-            int a = lower_bound_i(g.ent_iy0, e0, e1, u - (kTaps - 1));
-            int c = lower_bound_i(g.ent_iy0, a, e1, u + 1);
-            for (int e = a; e < c; ++e) {
-                int jt = __ldg(&g.ent_jt[e]);
-                int j = jt >> 4, t0 = jt & 15;
-                int d = u - __ldg(&g.ent_iy0[e]);
-                float coef = __ldg(&g.phix[(size_t)j * kTaps + t0]) * __ldg(&g.phiy[(size_t)j * kTaps + d]);
-                const float2 *fj = fg + (size_t)j * B;
-#pragma unroll
-                for (int b = 0; b < 8; ++b) {
-                    if (b < B) {
-                        float2 v = __ldg(&fj[b]);
-                        acc[b].x = fmaf(v.x, coef, acc[b].x);
-                        acc[b].y = fmaf(v.y, coef, acc[b].y);
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int b = 0; b < 8; ++b)
-            if (b < B) s[y * B + b] = acc[b];
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (key[mid] < v) lo = mid + 1;
+        else hi = mid;
     }
-    __syncthreads();
-    fft_smem(s, n, g.lg1, B, g.tw1, +1.f);
-    const size_t obase = ((size_t)grp * g.n0 + x) * N1 * B;
-    for (int idx = threadIdx.x; idx < N1 * B; idx += blockDim.x) {
-        int b = idx % B, Y = idx / B;
-        int y = (Y + n - N1 / 2) % n;
-        G1[obase + idx] = s[y * B + b];
+    return lo;
+}
+
+// Entries of a row staged at a time by the adjoint gather, and the padded
+// stride of a staged phiy window (so that neighbouring windows fall in
+// different shared-memory banks).
+constexpr int kChunk = 192;
+constexpr int kLdPs = 20;
+
+// Entries of grid row x whose first y tap r0 (in the rotated buffer with a
+// halo of kHalo rows on each side, r0 = iy0 + n1/2 + kHalo) is below v, for
+// v = 0..n1+16: [x][n1 + 17] counts relative to the row's first entry.
+__host__ __device__ inline int lb_ld(int n1) { return n1 + 2 * kHalo + 1; }
+
+// Shared-memory bytes of k_ypass_adj: the rotated row (padded stride), one
+// chunk of staged entries (phix*f values, phiy window, r0) and the row's
+// lower-bound table.
+__host__ __device__ inline size_t ypass_adj_smem(int n1, int B)
+{
+    size_t sb = (B == 8) ? 10 : (B == 4) ? 6 : B;
+    return (size_t)n1 * sb * sizeof(float2) +
+           (size_t)kChunk * (sb * sizeof(float2) + kLdPs * sizeof(float) + sizeof(int)) +
+           (((size_t)lb_ld(n1) * sizeof(unsigned short) + 15) & ~(size_t)15);
+}
+
+// Adds the staged entries with r0 in [i - 13, i] to acc: entry e puts
+// phiy_e[i - r0_e] * (phix * f)_e on buffer row i.  lb holds the row's
+// lower-bound table, off the index of the chunk's first entry in the row.
+template <int B, int SB>
+__device__ __forceinline__ void gather_row(int i, const unsigned short *lb, int off, int cn, const float2 *Qs,
+                                           const float *Ps, const int *Rs, float2 (&acc)[B])
+{
+    int lo = min(max((int)lb[max(i - (kTaps - 1), 0)] - off, 0), cn);
+    int hi = min(max((int)lb[i + 1] - off, 0), cn);
+    for (int e = lo; e < hi; ++e) {
+        float p = Ps[e * kLdPs + (i - Rs[e])];
+        float2 q[B];
+        load_b<B>(Qs + e * SB, q);
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            acc[b].x = fmaf(q[b].x, p, acc[b].x);
+            acc[b].y = fmaf(q[b].y, p, acc[b].y);
+        }
     }
 }
 
-// -------------------------------------------------------------- K1T ----
-// Adjoint x-pass: inverse FFT along x of column Y, crop X < N0 with
-// x = (X + n0 - N0/2) % n0, divide by ck = cx[X]*cy[Y] (NU:1104-1121).
-// MODE 0: out = fhat.  MODE 1: out = fhat - Ahwb (complexMinusCU,
-// NU:1563-1573) and per-slice partial sums of |out|^2 in double (alpha0,
-// NU:1641-1650) into part[G][N1][B].  out/Ahwb: [G][N1][N0][B].
-template <int MODE>
-__global__ void __launch_bounds__(1024) k_xpass_adj(Geo g, const float2 *__restrict__ G1, float2 *__restrict__ out,
-                            const float2 *__restrict__ Ahwb, double *__restrict__ part)
+// -------------------------------------------------------------- K2T ----
+// Adjoint y-pass.  Entry e (node j, x tap t0) of row x adds
+// phiy[j][t1] * phix[j][t0] * f_j to the rotated buffer row r0_e + t1,
+// t1 = 0..13; the reference sums the same terms per grid point through its
+// host-built CSR (NU:1078-1102).  Here a thread owns whole buffer rows and
+// gathers: entries are sorted by r0, so those covering row i are the
+// contiguous range r0 in [i - 13, i], read from the precomputed lower-bound
+// table.  The 8 halo rows on each side alias rows n-8..n-1 and 0..7, so
+// those rows also gather the range of their alias.  Entries are staged in
+// chunks (phix*f, phiy window, r0); a row's partial sum stays in its own
+// buffer row between chunks, so only the staging needs barriers and every
+// row gets its terms in a fixed order, with no atomics.  Then the inverse FFT
+// along y (NU:1203) reads the rotated row, and its last pass writes the rows
+// Y < N1 of the crop (NU:1104-1121: y = (Y + n1 - N1/2) % n1) straight to
+// G1[x][Y][b].  blockDim.x is max(32, n1*B/E); GUARD when that is more than
+// the FFT's n1*B/E threads.
+template <int B, int E, bool GUARD>
+__global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, float2 *__restrict__ G1)
 {
     extern __shared__ float2 s[];
-    double *red = (double *)(s + (size_t)g.n0 * g.B);
-    const int Y = blockIdx.x, grp = blockIdx.y, B = g.B, n = g.n0, N0 = g.N0;
-    const size_t ibase = (size_t)grp * n * g.N1 * B;
-    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
-        int b = idx % B, x = idx / B;
-        s[idx] = G1[ibase + ((size_t)x * g.N1 + Y) * B + b];
-    }
-    __syncthreads();
-    fft_smem(s, n, g.lg0, B, g.tw0, +1.f);
-    const float cyY = g.cy[Y];
-    const size_t obase = ((size_t)grp * g.N1 + Y) * N0 * B;
-    double acc2 = 0.0;
-    for (int idx = threadIdx.x; idx < N0 * B; idx += blockDim.x) {
-        int b = idx % B, X = idx / B;
-        int x = (X + n - N0 / 2) % n;
-        float ck = g.cx[X] * cyY;
-        float2 v = s[x * B + b];
-        v.x = v.x / ck;
-        v.y = v.y / ck;
-        if (MODE == 1) {
-            float2 a = Ahwb[obase + idx];
-            v.x = v.x - a.x;
-            v.y = v.y - a.y;
-            acc2 += (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+    constexpr int SB = RowStride<B>::v;
+    const int x = blockIdx.x, grp = blockIdx.y, n = g.n1, N1 = g.N1;
+    float2 *Qs = s + (size_t)n * SB;                           // [kChunk][SB]
+    float *Ps = reinterpret_cast<float *>(Qs + kChunk * SB);   // [kChunk][kLdPs]
+    int *Rs = reinterpret_cast<int *>(Ps + kChunk * kLdPs);    // [kChunk]
+    unsigned short *lb = reinterpret_cast<unsigned short *>(Rs + kChunk);
+    const int e0 = g.row_off[x], e1 = g.row_off[x + 1];
+    const float2 *fg = f + (size_t)grp * g.M * B;
+    const int T = blockDim.x, ldl = lb_ld(n);
+    const int r0ofs = n / 2 + kHalo;
+    for (int v = threadIdx.x; v < ldl; v += T) lb[v] = g.ent_lb[(size_t)x * ldl + v];
+    int c0 = e0;
+    do {
+        const int cn = min(kChunk, e1 - c0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cn; i += T) {
+            int jt = __ldg(&g.ent_jt[c0 + i]);
+            int j = jt >> 4, t0 = jt & 15;
+            float px = __ldg(&g.phix[(size_t)j * kTaps + t0]);
+            float2 v[B];
+            load_b<B>(fg + (size_t)j * B, v);
+#pragma unroll
+            for (int b = 0; b < B; ++b) v[b] = make_float2(v[b].x * px, v[b].y * px);
+            store_b<B>(Qs + i * SB, v);
+            const float4 *py4 = reinterpret_cast<const float4 *>(g.phiy + (size_t)j * kLdPhiy);
+            float4 *dst = reinterpret_cast<float4 *>(Ps + i * kLdPs);
+#pragma unroll
+            for (int q = 0; q < kLdPhiy / 4; ++q) dst[q] = __ldg(&py4[q]);
+            Rs[i] = __ldg(&g.ent_iy0[c0 + i]) + r0ofs;
         }
-        out[obase + idx] = v;
-    }
+        __syncthreads();
+        const int off = c0 - e0;
+        for (int r = threadIdx.x; r < n; r += T) {
+            float2 acc[B];
+            if (off == 0) {
+#pragma unroll
+                for (int b = 0; b < B; ++b) acc[b] = make_float2(0.f, 0.f);
+            } else {
+                load_b<B>(s + (size_t)r * SB, acc);
+            }
+            gather_row<B, SB>(r + kHalo, lb, off, cn, Qs, Ps, Rs, acc);
+            if (r < kHalo) gather_row<B, SB>(r + kHalo + n, lb, off, cn, Qs, Ps, Rs, acc);
+            if (r >= n - kHalo) gather_row<B, SB>(r + kHalo - n, lb, off, cn, Qs, Ps, Rs, acc);
+            store_b<B>(s + (size_t)r * SB, acc);
+        }
+        c0 += kChunk;
+    } while (c0 < e1);
+    __syncthreads();
+    float2 *row = s;
+    float2 *out = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
+    auto ld = [=](int q, int b) -> float2 { return row[q * SB + b]; };
+    auto st = [=](int kq, int b, float2 v) {
+        int Y = (kq + N1 / 2) & (n - 1);
+        if (Y < N1) out[(size_t)Y * B + b] = (kq & 1) ? make_float2(-v.x, -v.y) : v;   // undoes the rotation
+    };
+    fft_fused<B, SB, E, GUARD>(row, n, g.lg1, g.tw1, +1.f, ld, st);
+}
+
+// -------------------------------------------------------------- K1T ----
+// Adjoint x-pass: inverse FFT along x of column Y (first pass reads G1), and
+// the last pass crops X < N0 with x = (X + n0 - N0/2) % n0 and divides by
+// ck = cx[X]*cy[Y] (NU:1104-1121).  MODE 0: out = fhat.  MODE 1: out = fhat -
+// Ahwb (complexMinusCU, NU:1563-1573) and per-slice partial sums of |out|^2 in
+// double (alpha0, NU:1641-1650) into part[G][N1][B].  out/Ahwb: [G][N1][N0][B].
+template <int MODE, int B, int E>
+__global__ void FFT_BOUNDS(E) k_xpass_adj(Geo g, const float2 *__restrict__ G1, float2 *__restrict__ out,
+                                          const float2 *__restrict__ Ahwb, double *__restrict__ part)
+{
+    extern __shared__ float2 s[];
+    double *red = (double *)(s + (size_t)g.n0 * B);
+    const int Y = blockIdx.x, grp = blockIdx.y, n = g.n0, N0 = g.N0, N1 = g.N1;
+    const float2 *colin = G1 + (size_t)grp * n * N1 * B + (size_t)Y * B;
+    const float rcyY = g.rcy[Y];
+    const float *rcx = g.rcx;
+    const size_t obase = ((size_t)grp * N1 + Y) * N0 * B;
+    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) s[idx] = colin[(size_t)(idx / B) * N1 * B + (idx % B)];
+    __syncthreads();
+    auto ld = [=](int xq, int b) -> float2 { return s[xq * B + b]; };
+    struct Crop {
+        const float *rcx;
+        float rcyY;
+        int n, N0;
+        size_t obase;
+        const float2 *Ahwb;
+        float2 *out;
+        double acc2;
+        __device__ __forceinline__ void operator()(int k, int b, float2 v)
+        {
+            int X = (k + N0 / 2) & (n - 1);
+            if (X < N0) {
+                float r = rcx[X] * rcyY;
+                v.x = v.x * r;
+                v.y = v.y * r;
+                size_t o = obase + (size_t)X * B + b;
+                if (MODE == 1) {
+                    float2 a = Ahwb[o];
+                    v.x = v.x - a.x;
+                    v.y = v.y - a.y;
+                    acc2 += (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+                }
+                out[o] = v;
+            }
+        }
+    } st{rcx, rcyY, n, N0, obase, Ahwb, out, 0.0};
+    fft_fused<B, B, E>(s, n, g.lg0, g.tw0, +1.f, ld, st);
+    const double acc2 = st.acc2;
     if (MODE == 1) {
         double r = block_sum_per_slice(acc2, red, B);
-        if ((int)threadIdx.x < B) part[((size_t)grp * g.N1 + Y) * B + threadIdx.x] = r;
+        if ((int)threadIdx.x < B) part[((size_t)grp * N1 + Y) * B + threadIdx.x] = r;
     }
 }
 
@@ -298,36 +476,36 @@ __global__ void __launch_bounds__(1024) k_xpass_adj(Geo g, const float2 *__restr
 // (cunfft_trafo_1d NU:1479-1516: pre-pass NU:1432-1452, FFT, interpolation
 // NU:1454-1477 with taps summed in order), then f = b*w (NU:1539-1549).
 // rows: [S][nz][nx] (caller layout).  f, bout: [G][M][B]; bout may be null.
-__global__ void __launch_bounds__(1024) k_rows_fwd(Geo g, Geo1 g1, const float *__restrict__ rows, int S, float2 *__restrict__ f,
-                           float2 *__restrict__ bout)
+template <int B, int E>
+__global__ void FFT_BOUNDS(E) k_rows_fwd(Geo g, Geo1 g1, const float *__restrict__ rows, int S,
+                                         float2 *__restrict__ f, float2 *__restrict__ bout)
 {
     extern __shared__ float2 s[];
-    const int i = blockIdx.x, grp = blockIdx.y, B = g.B, n = g.n0, N = g.nx;
-    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) {
-        int b = idx % B, x = idx / B;
-        int X = (x + N / 2) % n;
+    constexpr int LB = Log2B<B>::v;
+    const int i = blockIdx.x, grp = blockIdx.y, n = g.n0, N = g.nx, nz = g.nz;
+    const float *rcx = g.rcx;
+    for (int idx = threadIdx.x; idx < N * B; idx += blockDim.x) {
+        int b = idx / N, X = idx % N;                      // coalesced along X
         int sl = grp * B + b;
-        float2 v = make_float2(0.f, 0.f);
-        if (X < N && sl < S) {
-            float c = g.cx[X];
-            v.x = rows[((size_t)sl * g.nz + i) * N + X] / c;
-            v.y = 0.f / c;
-        }
-        s[idx] = v;
+        s[X * B + b] = make_float2(sl < S ? rows[((size_t)sl * nz + i) * N + X] * rcx[X] : 0.f, 0.f);
     }
     __syncthreads();
-    fft_smem(s, n, g.lg0, B, g.tw0, -1.f);
+    auto ld = [=](int x, int b) -> float2 {
+        int X = (x + N / 2) & (n - 1);
+        return (X < N) ? s[X * B + b] : make_float2(0.f, 0.f);
+    };
+    auto st = [=](int k, int b, float2 v) { s[k * B + b] = v; };
+    fft_fused<B, B, E>(s, n, g.lg0, g.tw0, -1.f, ld, st);
+    __syncthreads();
     for (int idx = threadIdx.x; idx < N * B; idx += blockDim.x) {
-        int b = idx % B, k = idx / B;
+        int b = idx & (B - 1), k = idx >> LB;
         int l0 = __ldg(&g1.i10[k]);
         float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
         for (int t = 0; t < kTaps; ++t) {
-            int x = l0 + t;
-            x += (x < 0) ? n : 0;
-            x -= (x >= n) ? n : 0;
+            int xq = (l0 + t) & (n - 1);
             float p = __ldg(&g1.phi1[(size_t)k * kTaps + t]);
-            float2 v = s[x * B + b];
+            float2 v = s[xq * B + b];
             acc.x = fmaf(v.x, p, acc.x);
             acc.y = fmaf(v.y, p, acc.y);
         }
@@ -343,15 +521,16 @@ __global__ void __launch_bounds__(1024) k_rows_fwd(Geo g, Geo1 g1, const float *
 // NU:1518-1536): gather in node order (the order of the reference's 1-D CSR),
 // inverse FFT, crop, divide by the deapodisation, real part.
 // f: [G][nx][B]; out: [S][nx] (caller layout).
-__global__ void __launch_bounds__(1024) k_row_adj(Geo g, Geo1 g1, const float2 *__restrict__ f, float *__restrict__ out, int S)
+template <int B, int E>
+__global__ void FFT_BOUNDS(E) k_row_adj(Geo g, Geo1 g1, const float2 *__restrict__ f, float *__restrict__ out, int S)
 {
     extern __shared__ float2 s[];
-    const int grp = blockIdx.x, B = g.B, n = g.n0, N = g.nx;
+    const int grp = blockIdx.x, n = g.n0, N = g.nx;
     const float2 *fg = f + (size_t)grp * N * B;
     for (int x = threadIdx.x; x < n; x += blockDim.x) {
-        float2 acc[8];
+        float2 acc[B];
 #pragma unroll
-        for (int b = 0; b < 8; ++b) acc[b] = make_float2(0.f, 0.f);
+        for (int b = 0; b < B; ++b) acc[b] = make_float2(0.f, 0.f);
 #pragma unroll
         for (int al = 0; al < 2; ++al) {
             int u = x - al * n;
@@ -360,28 +539,26 @@ __global__ void __launch_bounds__(1024) k_row_adj(Geo g, Geo1 g1, const float2 *
             for (int k = a; k < c; ++k) {
                 int d = u - __ldg(&g1.i10[k]);
                 float p = __ldg(&g1.phi1[(size_t)k * kTaps + d]);
+                float2 v[B];
+                load_b<B>(fg + (size_t)k * B, v);
 #pragma unroll
-                for (int b = 0; b < 8; ++b) {
-                    if (b < B) {
-                        float2 v = fg[(size_t)k * B + b];
-                        acc[b].x = fmaf(v.x, p, acc[b].x);
-                        acc[b].y = fmaf(v.y, p, acc[b].y);
-                    }
+                for (int b = 0; b < B; ++b) {
+                    acc[b].x = fmaf(v[b].x, p, acc[b].x);
+                    acc[b].y = fmaf(v[b].y, p, acc[b].y);
                 }
             }
         }
-#pragma unroll
-        for (int b = 0; b < 8; ++b)
-            if (b < B) s[x * B + b] = acc[b];
+        store_b<B>(s + x * B, acc);
     }
     __syncthreads();
-    fft_smem(s, n, g.lg0, B, g.tw0, +1.f);
-    for (int idx = threadIdx.x; idx < N * B; idx += blockDim.x) {
-        int b = idx % B, X = idx / B;
+    const float *rcx = g.rcx;
+    auto ld = [=](int q, int b) -> float2 { return s[q * B + b]; };
+    auto st = [=](int k, int b, float2 v) {
+        int X = (k + N / 2) & (n - 1);
         int sl = grp * B + b;
-        int x = (X + n - N / 2) % n;
-        if (sl < S) out[(size_t)sl * N + X] = s[x * B + b].x / g.cx[X];
-    }
+        if (X < N && sl < S) out[(size_t)sl * N + X] = v.x * rcx[X];
+    };
+    fft_fused<B, B, E>(s, n, g.lg0, g.tw0, +1.f, ld, st);
 }
 
 // ----------------------------------------------------- layout moves ----
@@ -417,6 +594,7 @@ __global__ void k_img_out(const T *__restrict__ src, T *__restrict__ dst, int S,
     }
 }
 
+#ifndef ICON_KERNELS_TEMPLATES_ONLY
 // Caller nodes [S][M] <-> batched [G][M][B].
 __global__ void k_nodes_in(const float2 *__restrict__ src, float2 *__restrict__ dst, int S, int M, int B, size_t total)
 {
@@ -466,16 +644,21 @@ __global__ void k_alpha(const double *__restrict__ part_rtr, int nr, const doubl
     }
 }
 
+#endif  // ICON_KERNELS_TEMPLATES_ONLY
+
 // m <- m - alpha*Re(rhat) computed in double and stored as float; ICON steps
 // also clamp (ICONUpdateCU_R NU:1597-1616, INFRUpdateCU_R NU:1630-1639).
-// m: [G][N1][N0][B] float, rhat: same layout float2.
-// per_group = N1*N0*B elements.
+// m: [G][N1][N0][B] float, rhat: same layout float2.  blockIdx.y = group.
+template <int B>
 __global__ void k_update(float *__restrict__ m, const float2 *__restrict__ rhat, const double *__restrict__ alpha,
-                         int B, size_t per_group, size_t total, int clamp, int data_type, float thr)
+                         int per_group, int clamp, int data_type, float thr)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        int sl = (int)(i / per_group) * B + (int)(i % B);
-        float v = (float)((double)m[i] - alpha[sl] * (double)rhat[i].x);
+    const int grp = blockIdx.y;
+    float *mg = m + (size_t)grp * per_group;
+    const float2 *rg = rhat + (size_t)grp * per_group;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < per_group; i += gridDim.x * blockDim.x) {
+        double a = alpha[grp * B + (i & (B - 1))];
+        float v = (float)((double)mg[i] - a * (double)rg[i].x);
         if (clamp) {
             if (data_type == 1) {
                 if (v > thr) v = thr;
@@ -483,7 +666,7 @@ __global__ void k_update(float *__restrict__ m, const float2 *__restrict__ rhat,
                 if (v < thr) v = thr;
             }
         }
-        m[i] = v;
+        mg[i] = v;
     }
 }
 

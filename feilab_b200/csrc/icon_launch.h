@@ -1,0 +1,33 @@
+// icon_launch.h -- host launchers of the batched FFT kernels, one explicit
+// instantiation per slice-group size B (icon_kern_b.cu is compiled once per B
+// so that the kernel variants build in parallel).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace icon {
+
+struct Geo;
+struct Geo1;
+
+template <int B>
+struct Launch {
+    static void xpass_fwd(bool real_in, int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
+                          const void *in, float2 *G1);
+    static void ypass_fwd(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const float2 *G1,
+                          float2 *P);
+    static void interp_fin(int mode, dim3 grid, cudaStream_t st, const Geo &g, const float2 *P, float2 *f, double *part);
+    static void ypass_adj(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const float2 *f,
+                          float2 *G1);
+    static void xpass_adj(int mode, int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
+                          const float2 *G1, float2 *out, const float2 *Ahwb, double *part);
+    static void rows_fwd(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const Geo1 &g1,
+                         const float *rows, int S, float2 *f, float2 *bout);
+    static void row_adj(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const Geo1 &g1,
+                        const float2 *f, float *out, int S);
+    static void update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat, const double *alpha, int per_group,
+                       int clamp, int data_type, float thr);
+    // Raises the dynamic shared-memory limit of every kernel variant a plan uses.
+    static cudaError_t set_smem(int ex, int ey, size_t smem_x, size_t need_x, size_t smem_y, size_t smem_ya);
+};
+
+}  // namespace icon

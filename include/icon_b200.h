@@ -85,6 +85,9 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out);
  * NU:1393-1408, destroyGICONPara NU:1774-1787).  Synchronises the device. */
 icon_status icon_plan_destroy(icon_plan *plan);
 
+/* Angle (as in the .tlt file) at which icon_reconstruct_host reprojects. */
+icon_status icon_plan_set_reprojection(icon_plan *plan, float tilt_deg);
+
 /* dims[0..9] = N0, N1, n0, n1, M, ntilt, slices per group B, capacity,
  * device bytes held by the plan (low 31 bits in MiB), tilt index of the
  * smallest |angle| (the reprojection tilt of MainCode.cu:46-49). */
@@ -133,7 +136,10 @@ icon_status icon_reproject(icon_plan *plan, const float *d_m, float tilt_deg, fl
 
 /* The whole per-slice pipeline of Lib_2D2 (MainCode.cu:113-142) for S
  * slices from host memory: rows in, reconstructed slices out, plus the
- * reprojection at the smallest-|angle| tilt when h_reproj is not NULL.
+ * reprojection when h_reproj is not NULL -- at the smallest-|angle| tilt of
+ * the plan (MainCode.cu:46-49, :142) unless icon_plan_set_reprojection chose
+ * another angle (the cross-validation solve of MainCode_crossV.cu:153
+ * reprojects at the tilt it left out).
  * Host buffers should be pinned for full copy speed.  Work is queued on
  * `stream` (NULL: a stream of its own); the call returns after the results
  * are in host memory.  S may exceed the capacity: it is processed in chunks. */
@@ -175,6 +181,12 @@ icon_status icon_rows_forward_noalloc(const float *d_rows, int nx, int ntilt, in
 
 /* Message for the last failed call on this thread ("" if none). */
 const char *icon_last_error(void);
+
+/* Number of CUDA devices and, for the first `max` of them, their
+ * multiprocessor counts (h_sm may be NULL).  The reference queries the same to
+ * split slices across GPUs in proportion to SM count (ICONGPU.cu:153-160,
+ * :398-430). */
+icon_status icon_devices(int *h_count, int *h_sm, int max);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,109 @@
+"""The icon-gpu command-line tool against the reference ICON-GPU run.
+
+The golden "cli" case holds what the reference tool wrote for a 64-pixel,
+25-tilt stack (slices 0..3, thickness 40, -iter 1,5,1): the slice files
+reconstruction/midNNNNN.mrc (ICONGPU.cu:330-366, saveMRC_real.cu:33-56) and the
+crossValidation outputs (GroundTruth / reprojection MRCs and the smoothed FRC
+curves, ICONGPU.cu:468-592).  The same stack and tilt file are written here,
+the tool is run on them and every file is compared: headers field by field,
+data within the solve tolerance, FRC curves within an absolute tolerance.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+TOOL = os.path.join(ROOT, "feilab_b200", "icon-gpu")
+TOL_SOLVE = 1e-4      # relative L2, as the solve parity tests
+TOL_FRC = 2e-3        # absolute, per FRC ring
+STAT_FIELDS = ("amin", "amax", "amean", "rms")
+
+
+def _run(args, cwd):
+    return subprocess.run([TOOL] + args, cwd=cwd, capture_output=True, text=True, timeout=300)
+
+
+def _mrc_from_bytes(raw, tmp_path, name):
+    from feilab_b200 import mrc
+    p = tmp_path / name
+    p.write_bytes(raw)
+    return mrc.read(str(p))
+
+
+def _compare_headers(h, hr):
+    for f in h.dtype.names:
+        if f in STAT_FIELDS:
+            np.testing.assert_allclose(float(h[f]), float(hr[f]), rtol=1e-3, atol=1e-5, err_msg=f)
+        else:
+            assert np.array_equal(h[f], hr[f]), f
+
+
+def test_cli_usage_errors(tmp_path):
+    p = _run(["-i", "missing.mrc"], str(tmp_path))
+    assert p.returncode != 0
+    assert "parameter error!" in p.stdout
+
+
+@pytest.mark.gpu
+def test_cli_matches_reference_tool(golden, tmp_path):
+    from feilab_b200 import mrc
+    z = golden["cli"]
+    nx, th, S = int(z["nx"]), int(z["thickness"]), int(z["S"])
+    stack, tlt, out = tmp_path / "stack.mrc", tmp_path / "cli.tlt", tmp_path / "res"
+    mrc.write_tilt_series(str(stack), z["rows"])
+    mrc.write_tlt(str(tlt), z["tilts"])
+    out.mkdir()
+    a, b, c = (int(v) for v in z["sched"])
+    p = _run(["-i", str(stack), "-t", str(tlt), "-o", str(out), "-s", f"0,{S - 1}", "-iter", f"{a},{b},{c}",
+              "-d", str(int(z["data_type"])), "-thr", str(float(z["threshold"])), "-g", "0", "-thi", str(th)],
+             str(tmp_path))
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert "ICON-GPU finish!" in p.stdout
+    for s in range(S):
+        assert f"slice {s} finished" in p.stdout
+        h, d = mrc.read(str(out / "reconstruction" / f"mid{s:05d}.mrc"))
+        hr, dr = _mrc_from_bytes(z[f"cli_mid{s:05d}"].tobytes(), tmp_path, f"ref{s}.mrc")
+        _compare_headers(h, hr)
+        assert d.shape == dr.shape == (1, th, nx)
+        assert rel_l2(d[0], dr[0]) < TOL_SOLVE, s
+    for fn in ("GroundTruth.mrc", "fullRec_reProjection.mrc", "crossV_reprojection.mrc"):
+        h, d = mrc.read(str(out / "crossValidation" / fn))
+        hr, dr = _mrc_from_bytes(z["cli_" + fn.replace(".", "_")].tobytes(), tmp_path, "ref_" + fn)
+        _compare_headers(h, hr)
+        assert d.shape == dr.shape
+        if fn == "GroundTruth.mrc":
+            np.testing.assert_array_equal(d, dr)
+        else:
+            assert rel_l2(d, dr) < TOL_SOLVE, fn
+    for fn in ("fullRec.frc", "crossV.frc"):
+        got = np.loadtxt(str(out / "crossValidation" / fn))
+        ref = np.loadtxt(z["cli_" + fn.replace(".", "_")].tobytes().decode().splitlines())
+        assert got.shape == ref.shape == (nx // 2, 2)
+        np.testing.assert_array_equal(got[:, 0], ref[:, 0])
+        np.testing.assert_allclose(got[:, 1], ref[:, 1], atol=TOL_FRC, err_msg=fn)
+
+
+@pytest.mark.gpu
+def test_cli_volume_output(golden, tmp_path):
+    # --volume writes the slices as one MRC (sections = slices, X fastest), the
+    # same values as the per-slice files.
+    from feilab_b200 import mrc
+    z = golden["cli"]
+    nx, th, S = int(z["nx"]), int(z["thickness"]), int(z["S"])
+    stack, tlt, out = tmp_path / "stack.mrc", tmp_path / "cli.tlt", tmp_path / "res"
+    mrc.write_tilt_series(str(stack), z["rows"])
+    mrc.write_tlt(str(tlt), z["tilts"])
+    out.mkdir()
+    vol = tmp_path / "vol.mrc"
+    p = _run(["-i", str(stack), "-t", str(tlt), "-o", str(out), "-s", f"0,{S - 1}", "-iter", "1,5,1", "-d", "2",
+              "-thr", "0", "-g", "0", "-thi", str(th), "-skipCV", "1", "--volume", str(vol)], str(tmp_path))
+    assert p.returncode == 0, p.stdout + p.stderr
+    h, v = mrc.read(str(vol))
+    assert v.shape == (S, th, nx)
+    for s in range(S):
+        _, d = mrc.read(str(out / "reconstruction" / f"mid{s:05d}.mrc"))
+        np.testing.assert_array_equal(v[s], d[0])
