@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -164,6 +165,7 @@ struct NodeTables {
     float *phix = nullptr, *phiy = nullptr, *w = nullptr;
     int *ix0 = nullptr, *iy0 = nullptr, *row_off = nullptr, *ent_jt = nullptr, *ent_iy0 = nullptr;
     unsigned short *ent_lb = nullptr;
+    float *ent_phiy = nullptr, *ent_pxy = nullptr;
 };
 
 }  // namespace
@@ -228,7 +230,7 @@ struct icon_plan {
         g.M = t.M; g.nx = nx; g.nz = nz; g.B = B;
         g.w = t.w; g.phix = t.phix; g.phiy = t.phiy; g.ix0 = t.ix0; g.iy0 = t.iy0;
         g.cx = cx; g.cy = cy; g.rcx = rcx; g.rcy = rcy; g.row_off = t.row_off; g.ent_jt = t.ent_jt; g.ent_iy0 = t.ent_iy0;
-        g.ent_lb = t.ent_lb;
+        g.ent_lb = t.ent_lb; g.ent_phiy = t.ent_phiy; g.ent_pxy = t.ent_pxy;
         g.tw0 = tw0; g.tw1 = tw1;
         return g;
     }
@@ -357,13 +359,17 @@ icon_status build_tables(icon_plan *p, const float *xy, const float *w, int M, N
             while (e < c && ky2[e] + r0ofs < v) ++e;
             lb[(size_t)x * ldl + v] = (unsigned short)(e - a);
         }
-        if (c > a && (ky2[a] + r0ofs < 0 || ky2[c - 1] + r0ofs + kTaps > ldl - 1))
+        if (c > a && (ky2[a] + r0ofs < 0 || ky2[c - 1] + r0ofs + kTaps > p->n1 + 2 * icon::kHalo))
             return fail(ICON_ERR_INVALID, "window taps outside the rotated y buffer");
     }
     ICON_TRY(p->arena.upload(&t.row_off, cnt.data(), (size_t)n0 + 1));
     ICON_TRY(p->arena.upload(&t.ent_jt, jt2.data(), E));
     ICON_TRY(p->arena.upload(&t.ent_iy0, ky2.data(), E));
     ICON_TRY(p->arena.upload(&t.ent_lb, lb.data(), lb.size()));
+    ICON_TRY(p->arena.alloc(&t.ent_phiy, E * icon::kLdPhiy));
+    ICON_TRY(p->arena.alloc(&t.ent_pxy, E * icon::kLdPhiy));
+    icon::k_entry_tables<<<(unsigned)((E + 255) / 256), 256>>>(t.ent_jt, (int)E, t.phiy, t.phix, t.ent_phiy, t.ent_pxy);
+    ICON_CUDA(cudaGetLastError());
     ICON_TRY(p->arena.upload(&t.w, w, (size_t)M));
     return ICON_OK;
 }
@@ -412,7 +418,7 @@ icon_status launch_forward(icon_plan *p, const NodeTables &t, const void *img_in
     Geo g = p->geo(t);
     const StageBytes sb = stage_bytes(p, t);
     const double slots = (double)G * p->B;
-    dim3 gx(p->N1, G), gy(p->n0, G);
+    dim3 gx(p->N1, G), gy(G, p->n0);
     WITH_B(p->B,
         LAUNCH_B(p, K_XF, st, (real_in ? sb.xf_real : sb.xf_cplx) * slots,
                  L::xpass_fwd(real_in, p->ex, gx, p->thr_x, p->smem_x, st, g, img_int, p->G1));
@@ -431,7 +437,7 @@ icon_status launch_adjoint(icon_plan *p, const float2 *f_int, int G, int mode, f
     Geo g = p->geo(p->nodes);
     const StageBytes sb = stage_bytes(p, p->nodes);
     const double slots = (double)G * p->B;
-    dim3 gy(p->n0, G), gx(p->N1, G);
+    dim3 gy(G, p->n0), gx(p->N1, G);
     size_t smem = p->smem_x + sizeof(double) * p->thr_x;
     WITH_B(p->B,
         LAUNCH_B(p, K_YA, st, sb.ya * slots, L::ypass_adj(p->ey, gy, p->thr_y, p->smem_ya, st, g, f_int, p->G1));
@@ -551,6 +557,11 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
     p->lg1 = ilog2(p->n1);
     int nmax = std::max(p->n0, p->n1);
     int B = nmax <= 2048 ? 8 : (nmax <= 4096 ? 4 : 2);
+    // ICON_BATCH=1|2|4|8 lowers the slices per group, for tuning.
+    if (const char *ov = std::getenv("ICON_BATCH")) {
+        int v = atoi(ov);
+        if ((v == 1 || v == 2 || v == 4 || v == 8) && v < B) B = v;
+    }
     while (B > 1 && B / 2 >= geo->capacity) B /= 2;
     p->B = B;
     p->cap = geo->capacity;
@@ -600,10 +611,18 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
     };
     p->ex = pick_e(p->lg0, p->n0);
     p->ey = pick_e(p->lg1, p->n1);
+    // ICON_FFT_E="ex,ey" (each 16 or 32) overrides the choice, for tuning.
+    if (const char *ov = std::getenv("ICON_FFT_E")) {
+        int a = 0, c = 0;
+        if (sscanf(ov, "%d,%d", &a, &c) == 2) {
+            if ((a == 16 || a == 32) && p->n0 * B >= a * 32) p->ex = a;
+            if ((c == 16 || c == 32) && p->n1 * B >= c * 32) p->ey = c;
+        }
+    }
     p->thr_x = p->n0 * B / p->ex;
     p->thr_y = p->n1 * B / p->ey;
     p->smem_x = (size_t)p->n0 * B * sizeof(float2);
-    p->smem_y = ybuf_bytes(p->n1, B);
+    p->smem_y = ybuf_bytes(p->n1, B) + icon::ypass_fwd_pre_bytes();
     p->smem_ya = icon::ypass_adj_smem(p->n1, B);
     int smem_max = 0;
     ICON_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));

@@ -282,14 +282,26 @@ __device__ __forceinline__ void fpass(float2 *s, int n, int Ns, const float2 *__
             int item = threadIdx.x + q * T;
             int b = item & (B - 1), j = item >> LB;
             int k = j & (Ns - 1);
+            // Inter-pass twiddle w^(r k step), w = exp(-dir 2 pi i / n): read
+            // from the table for r = 0, 8, 16, 24 and stepped by w^(k step)
+            // in between (at most 7 products from a table value).
+            float2 w1 = make_float2(1.f, 0.f), w = w1;
+            if (!FIRST && Ns > 1) {
+                w1 = __ldg(&tw[k * step]);
+                w1.y = -dir * w1.y;
+            }
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 float2 x;
                 if constexpr (FIRST) x = ld(j + r * nb, b);
                 else x = s[(j + r * nb) * SB + b];
                 if (!FIRST && r > 0 && Ns > 1) {
-                    float2 w = __ldg(&tw[r * k * step]);
-                    w.y = -dir * w.y;
+                    if ((r & 7) == 0) {
+                        w = __ldg(&tw[r * k * step]);
+                        w.y = -dir * w.y;
+                    } else {
+                        w = (r & 7) == 1 ? ((r == 1) ? w1 : cmul(w, w1)) : cmul(w, w1);
+                    }
                     x = cmul(x, w);
                 }
                 v[q][brev5(r) >> (5 - Lg<R>::v)] = x;
@@ -365,6 +377,45 @@ __device__ __forceinline__ void fft_fused(float2 *s, int n, int lg, const float2
 
 // Row stride (in float2) of the gather buffers: padded so that 16-byte loads
 // of eight neighbouring rows fall in different banks.
+// Asynchronous global -> shared copies (cp.async): the copies of a thread
+// are all in flight at once; commit_group closes a group, wait_group<N>
+// waits until at most N of the thread's groups are pending.
+__device__ __forceinline__ unsigned smem_addr(const void *p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async(void *dst, const void *src)
+{
+    static_assert(N == 4 || N == 8 || N == 16, "cp.async copies 4, 8 or 16 bytes");
+    if constexpr (N == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_addr(dst)), "l"(src), "n"(N) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Block-wide asynchronous copy of `bytes` (a multiple of 4) in the widest
+// units that the two addresses and the size allow.
+__device__ __forceinline__ void copy_async(void *dst, const void *src, size_t bytes)
+{
+    const size_t al = (size_t)dst | (size_t)src | bytes;
+    char *d = static_cast<char *>(dst);
+    const char *s = static_cast<const char *>(src);
+    if ((al & 15) == 0) {
+        for (size_t o = (size_t)threadIdx.x * 16; o < bytes; o += (size_t)blockDim.x * 16) cp_async<16>(d + o, s + o);
+    } else if ((al & 7) == 0) {
+        for (size_t o = (size_t)threadIdx.x * 8; o < bytes; o += (size_t)blockDim.x * 8) cp_async<8>(d + o, s + o);
+    } else {
+        for (size_t o = (size_t)threadIdx.x * 4; o < bytes; o += (size_t)blockDim.x * 4) cp_async<4>(d + o, s + o);
+    }
+}
+
 template <int B>
 struct RowStride {
     static constexpr int v = (B == 8) ? 10 : (B == 4) ? 6 : B;

@@ -53,6 +53,8 @@ struct Geo {
     const int *ent_jt;     // [M*14] entry: node*16 + x tap, sorted by (row, iy0, node)
     const int *ent_iy0;    // [M*14] iy0 of the entry's node (sort key within a row)
     const unsigned short *ent_lb;   // [n0][n1+17] per-row lower bounds of r0 (k_ypass_adj)
+    const float *ent_phiy; // [M*14][16] phiy of the entry's node, in entry order
+    const float *ent_pxy;  // [M*14][16] phix[j][t0] * phiy[j][t1], in entry order
     const float2 *tw0;     // [n0] exp(-2 pi i q / n0)
     const float2 *tw1;     // [n1] exp(-2 pi i q / n1)
 };
@@ -83,6 +85,25 @@ __global__ void k_window(const float *__restrict__ x, int stride, int M, int n, 
         phi[(size_t)j * ld + t] = bf * expf(-((n * x1) * (n * x1) / b));
     }
     for (int t = kTaps; t < ld; ++t) phi[(size_t)j * ld + t] = 0.f;
+}
+
+// Window values copied into entry order (entry e = node j, x tap t0), so the
+// y-passes read them as contiguous streams: ephiy[e] = phiy[j] (16 floats)
+// and epxy[e][t1] = phix[j][t0] * phiy[j][t1], the product the reference's
+// adjoint CSR stores per grid point and node (NU:44-218).
+__global__ void k_entry_tables(const int *__restrict__ jt, int E, const float *__restrict__ phiy,
+                               const float *__restrict__ phix, float *__restrict__ ephiy, float *__restrict__ epxy)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    int v = jt[e], j = v >> 4, t0 = v & 15;
+    const float px = phix[(size_t)j * kTaps + t0];
+#pragma unroll
+    for (int t = 0; t < kLdPhiy; ++t) {
+        float py = phiy[(size_t)j * kLdPhiy + t];
+        ephiy[(size_t)e * kLdPhiy + t] = py;
+        epxy[(size_t)e * kLdPhiy + t] = px * py;
+    }
 }
 
 #endif  // ICON_KERNELS_TEMPLATES_ONLY
@@ -137,22 +158,24 @@ __global__ void FFT_BOUNDS(E) k_xpass_fwd(Geo g, const void *__restrict__ in, fl
     const float *rcx = g.rcx;
     const size_t ibase = ((size_t)grp * N1 + Y) * N0 * B;
     float2 *out = G1 + (size_t)grp * n * N1 * B + (size_t)Y * B;
-    // Stage the deapodised column [N0][B] (contiguous in global memory); the
-    // first FFT pass reads it before anything is written to s.
-    for (int idx = threadIdx.x; idx < N0 * B; idx += blockDim.x) {
-        float r = rcx[idx / B] * rcyY;
-        float2 v;
-        if (REAL_IN) v = make_float2(((const float *)in)[ibase + idx] * r, 0.f);
-        else {
-            float2 t = ((const float2 *)in)[ibase + idx];
-            v = make_float2(t.x * r, t.y * r);
-        }
-        s[idx] = v;
-    }
+    // Copy the column [N0][B] (contiguous in global memory) and 1/cx behind
+    // it; the first FFT pass reads both, deapodising as it reads, before
+    // anything is written to s.
+    const size_t vbytes = REAL_IN ? sizeof(float) : sizeof(float2);
+    char *raw = reinterpret_cast<char *>(s);
+    float *rcs = reinterpret_cast<float *>(raw + (((size_t)N0 * B * vbytes + 15) & ~(size_t)15));
+    copy_async(raw, (const char *)in + ibase * vbytes, (size_t)N0 * B * vbytes);
+    copy_async(rcs, rcx, (size_t)N0 * sizeof(float));
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     auto ld = [=](int x, int b) -> float2 {
         int X = (x + N0 / 2) & (n - 1);
-        return (X < N0) ? s[X * B + b] : make_float2(0.f, 0.f);
+        if (X >= N0) return make_float2(0.f, 0.f);
+        float r = rcs[X] * rcyY;
+        if (REAL_IN) return make_float2(reinterpret_cast<const float *>(raw)[X * B + b] * r, 0.f);
+        float2 v = reinterpret_cast<const float2 *>(raw)[X * B + b];
+        return make_float2(v.x * r, v.y * r);
     };
     auto st = [=](int x, int b, float2 v) { out[(size_t)x * N1 * B + b] = v; };
     fft_fused<B, B, E>(s, n, g.lg0, g.tw0, -1.f, ld, st);
@@ -172,22 +195,50 @@ __device__ __forceinline__ void fill_halo(float2 *s, int n)
 }
 
 // --------------------------------------------------------------- K2 ----
+// Entries of a row whose tables k_ypass_fwd copies into shared memory before
+// its FFT (the copy overlaps the FFT); one record is the phiy window (16
+// floats), the node*16 + x tap and iy0.
+constexpr int kPreEntries = 256;
+constexpr int kPreRecord = kLdPhiy * 4 + 8;
+__host__ __device__ inline size_t ypass_fwd_pre_bytes() { return (size_t)kPreEntries * kPreRecord; }
+
 // Forward y-pass fused with the y-direction interpolation.  Row x of G1 holds
 // the N1 nonzero columns; column Y sits at y with (y + N1/2) % n1 == Y.
 // P[G][M][14][B]: P[j][t0] = sum_t1 phiy[j][t1] * G[x][(iy0_j + t1) mod n1],
 // x = (ix0_j + t0) mod n0.  (NU:669-727 sum the same 196 products per node.)
-// The first FFT pass reads G1 directly; one thread per entry computes all B
-// slices of it from the rotated row in shared memory.
+// The row is copied to shared memory and the tables of the row's first
+// entries are copied behind it; the FFT waits only for the row.  One thread
+// per entry then computes all B slices of it from the rotated row; entries
+// past the copied ones are loaded one round ahead.
 template <int B, int E>
 __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, float2 *__restrict__ P)
 {
     extern __shared__ float2 s[];
     constexpr int SB = RowStride<B>::v;
-    const int x = blockIdx.x, grp = blockIdx.y, n = g.n1, N1 = g.N1;
+    const int grp = blockIdx.x, x = blockIdx.y, n = g.n1, N1 = g.N1;
+    const int T = blockDim.x;
     const float2 *rowin = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
     float2 *row = s + kHalo * SB;
-    // Stage the N1 nonzero values of the row (contiguous in G1).
-    for (int idx = threadIdx.x; idx < N1 * B; idx += blockDim.x) row[idx] = rowin[idx];
+    float *pre_phi = reinterpret_cast<float *>(s + (size_t)(n + 2 * kHalo) * SB);   // [kPreEntries][16]
+    int *pre_jt = reinterpret_cast<int *>(pre_phi + kPreEntries * kLdPhiy);           // [kPreEntries]
+    int *pre_iy = pre_jt + kPreEntries;                                                 // [kPreEntries]
+    const int e0 = g.row_off[x], cnt = g.row_off[x + 1] - e0;
+    const int staged = min(cnt, min(T, kPreEntries));
+    // Group 1: the N1 nonzero values of the row (contiguous in G1).
+    copy_async(row, rowin, (size_t)N1 * B * sizeof(float2));
+    cp_async_commit();
+    // Group 2: tables of the first entries.
+    if ((int)threadIdx.x < staged) {
+        const int e = e0 + threadIdx.x;
+        const float *src = g.ent_phiy + (size_t)e * kLdPhiy;
+        float *dst = pre_phi + threadIdx.x * kLdPhiy;
+#pragma unroll
+        for (int q = 0; q < kLdPhiy / 4; ++q) cp_async<16>(dst + 4 * q, src + 4 * q);
+        cp_async<4>(pre_jt + threadIdx.x, g.ent_jt + e);
+        cp_async<4>(pre_iy + threadIdx.x, g.ent_iy0 + e);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
     auto ld = [=](int y, int b) -> float2 {
         int Y = (y + N1 / 2) & (n - 1);
@@ -196,25 +247,46 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
     };
     auto st = [=](int q, int b, float2 v) { row[q * SB + b] = v; };
     fft_fused<B, SB, E>(row, n, g.lg1, g.tw1, -1.f, ld, st);
+    cp_async_wait<0>();
     __syncthreads();
     fill_halo<B, SB>(s, n);
     __syncthreads();
-    const int e0 = g.row_off[x], e1 = g.row_off[x + 1];
     const size_t pbase = (size_t)grp * g.M * kTaps * B;
     const int rofs = n / 2 + kHalo;
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        int jt = __ldg(&g.ent_jt[e]);
-        int j = jt >> 4, t0 = jt & 15;
-        const float2 *sr = s + (__ldg(&g.ent_iy0[e]) + rofs) * SB;
-        const float4 *py4 = reinterpret_cast<const float4 *>(g.phiy + (size_t)j * kLdPhiy);
+    struct Ent {
+        int jt, iy;
+        float4 py[4];
+    };
+    auto load_global = [&](int e, Ent &r) {
+        r.jt = __ldg(&g.ent_jt[e]);
+        r.iy = __ldg(&g.ent_iy0[e]);
+        const float4 *py4 = reinterpret_cast<const float4 *>(g.ent_phiy + (size_t)e * kLdPhiy);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) r.py[q] = __ldg(&py4[q]);
+    };
+    int i = threadIdx.x;
+    Ent cur, nxt;
+    if (i < staged) {
+        cur.jt = pre_jt[i];
+        cur.iy = pre_iy[i];
+        const float4 *py4 = reinterpret_cast<const float4 *>(pre_phi + i * kLdPhiy);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cur.py[q] = py4[q];
+    } else if (i < cnt) {
+        load_global(e0 + i, cur);
+    }
+    while (i < cnt) {
+        const int i2 = i + T;             // never among the copied entries (staged <= T)
+        if (i2 < cnt) load_global(e0 + i2, nxt);
+        const int j = cur.jt >> 4, t0 = cur.jt & 15;
+        const float2 *sr = s + (cur.iy + rofs) * SB;
         float py[16];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            float4 t = __ldg(&py4[i]);
-            py[4 * i] = t.x;
-            py[4 * i + 1] = t.y;
-            py[4 * i + 2] = t.z;
-            py[4 * i + 3] = t.w;
+        for (int q = 0; q < 4; ++q) {
+            py[4 * q] = cur.py[q].x;
+            py[4 * q + 1] = cur.py[q].y;
+            py[4 * q + 2] = cur.py[q].z;
+            py[4 * q + 3] = cur.py[q].w;
         }
         float2 acc[B];
 #pragma unroll
@@ -230,6 +302,8 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
             }
         }
         store_b<B>(P + pbase + ((size_t)j * kTaps + t0) * B, acc);
+        cur = nxt;
+        i = i2;
     }
 }
 
@@ -304,11 +378,12 @@ constexpr int kLdPs = 20;
 
 // Entries of grid row x whose first y tap r0 (in the rotated buffer with a
 // halo of kHalo rows on each side, r0 = iy0 + n1/2 + kHalo) is below v, for
-// v = 0..n1+16: [x][n1 + 17] counts relative to the row's first entry.
-__host__ __device__ inline int lb_ld(int n1) { return n1 + 2 * kHalo + 1; }
+// v = 0..n1+16: [x][lb_ld] counts relative to the row's first entry, rows
+// padded to 16 bytes.
+__host__ __device__ inline int lb_ld(int n1) { return (n1 + 2 * kHalo + 1 + 7) & ~7; }
 
 // Shared-memory bytes of k_ypass_adj: the rotated row (padded stride), one
-// chunk of staged entries (phix*f values, phiy window, r0) and the row's
+// chunk of staged entries (f values, phix*phiy window, iy0) and the row's
 // lower-bound table.
 __host__ __device__ inline size_t ypass_adj_smem(int n1, int B)
 {
@@ -319,16 +394,17 @@ __host__ __device__ inline size_t ypass_adj_smem(int n1, int B)
 }
 
 // Adds the staged entries with r0 in [i - 13, i] to acc: entry e puts
-// phiy_e[i - r0_e] * (phix * f)_e on buffer row i.  lb holds the row's
+// (phix * phiy)_e[i - r0_e] * f_e on buffer row i (Rs holds iy0).  lb holds the row's
 // lower-bound table, off the index of the chunk's first entry in the row.
 template <int B, int SB>
-__device__ __forceinline__ void gather_row(int i, const unsigned short *lb, int off, int cn, const float2 *Qs,
-                                           const float *Ps, const int *Rs, float2 (&acc)[B])
+__device__ __forceinline__ void gather_row(int i, int r0ofs, const unsigned short *lb, int off, int cn,
+                                           const float2 *Qs, const float *Ps, const int *Rs, float2 (&acc)[B])
 {
     int lo = min(max((int)lb[max(i - (kTaps - 1), 0)] - off, 0), cn);
     int hi = min(max((int)lb[i + 1] - off, 0), cn);
+    const int iu = i - r0ofs;
     for (int e = lo; e < hi; ++e) {
-        float p = Ps[e * kLdPs + (i - Rs[e])];
+        float p = Ps[e * kLdPs + (iu - Rs[e])];   // i - r0 in 0..13, r0 = iy0 + r0ofs
         float2 q[B];
         load_b<B>(Qs + e * SB, q);
 #pragma unroll
@@ -347,10 +423,11 @@ __device__ __forceinline__ void gather_row(int i, const unsigned short *lb, int 
 // gathers: entries are sorted by r0, so those covering row i are the
 // contiguous range r0 in [i - 13, i], read from the precomputed lower-bound
 // table.  The 8 halo rows on each side alias rows n-8..n-1 and 0..7, so
-// those rows also gather the range of their alias.  Entries are staged in
-// chunks (phix*f, phiy window, r0); a row's partial sum stays in its own
-// buffer row between chunks, so only the staging needs barriers and every
-// row gets its terms in a fixed order, with no atomics.  Then the inverse FFT
+// those rows also gather the range of their alias.  Entries are copied in
+// chunks with cp.async (f_j, the phix*phiy window, iy0); a row's partial sum
+// stays in its own buffer row between chunks, so only the staging needs
+// barriers and every row gets its terms in a fixed order, with no atomics.
+// Then the inverse FFT
 // along y (NU:1203) reads the rotated row, and its last pass writes the rows
 // Y < N1 of the crop (NU:1104-1121: y = (Y + n1 - N1/2) % n1) straight to
 // G1[x][Y][b].  blockDim.x is max(32, n1*B/E); GUARD when that is more than
@@ -360,7 +437,7 @@ __global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, f
 {
     extern __shared__ float2 s[];
     constexpr int SB = RowStride<B>::v;
-    const int x = blockIdx.x, grp = blockIdx.y, n = g.n1, N1 = g.N1;
+    const int grp = blockIdx.x, x = blockIdx.y, n = g.n1, N1 = g.N1;
     float2 *Qs = s + (size_t)n * SB;                           // [kChunk][SB]
     float *Ps = reinterpret_cast<float *>(Qs + kChunk * SB);   // [kChunk][kLdPs]
     int *Rs = reinterpret_cast<int *>(Ps + kChunk * kLdPs);    // [kChunk]
@@ -369,26 +446,27 @@ __global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, f
     const float2 *fg = f + (size_t)grp * g.M * B;
     const int T = blockDim.x, ldl = lb_ld(n);
     const int r0ofs = n / 2 + kHalo;
-    for (int v = threadIdx.x; v < ldl; v += T) lb[v] = g.ent_lb[(size_t)x * ldl + v];
+    copy_async(lb, g.ent_lb + (size_t)x * ldl, (size_t)ldl * sizeof(unsigned short));   // waited for with chunk 0
     int c0 = e0;
     do {
         const int cn = min(kChunk, e1 - c0);
         __syncthreads();
         for (int i = threadIdx.x; i < cn; i += T) {
-            int jt = __ldg(&g.ent_jt[c0 + i]);
-            int j = jt >> 4, t0 = jt & 15;
-            float px = __ldg(&g.phix[(size_t)j * kTaps + t0]);
-            float2 v[B];
-            load_b<B>(fg + (size_t)j * B, v);
+            const int j = __ldg(&g.ent_jt[c0 + i]) >> 4;
+            const float2 *src = fg + (size_t)j * B;
+            if constexpr (B >= 2) {
 #pragma unroll
-            for (int b = 0; b < B; ++b) v[b] = make_float2(v[b].x * px, v[b].y * px);
-            store_b<B>(Qs + i * SB, v);
-            const float4 *py4 = reinterpret_cast<const float4 *>(g.phiy + (size_t)j * kLdPhiy);
-            float4 *dst = reinterpret_cast<float4 *>(Ps + i * kLdPs);
+                for (int q = 0; q < B / 2; ++q) cp_async<16>(Qs + i * SB + 2 * q, src + 2 * q);
+            } else {
+                cp_async<8>(Qs + i * SB, src);
+            }
+            const float *pxy = g.ent_pxy + (size_t)(c0 + i) * kLdPhiy;
 #pragma unroll
-            for (int q = 0; q < kLdPhiy / 4; ++q) dst[q] = __ldg(&py4[q]);
-            Rs[i] = __ldg(&g.ent_iy0[c0 + i]) + r0ofs;
+            for (int q = 0; q < kLdPhiy / 4; ++q) cp_async<16>(Ps + i * kLdPs + 4 * q, pxy + 4 * q);
+            cp_async<4>(Rs + i, g.ent_iy0 + c0 + i);
         }
+        cp_async_commit();
+        cp_async_wait<0>();
         __syncthreads();
         const int off = c0 - e0;
         for (int r = threadIdx.x; r < n; r += T) {
@@ -399,9 +477,9 @@ __global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, f
             } else {
                 load_b<B>(s + (size_t)r * SB, acc);
             }
-            gather_row<B, SB>(r + kHalo, lb, off, cn, Qs, Ps, Rs, acc);
-            if (r < kHalo) gather_row<B, SB>(r + kHalo + n, lb, off, cn, Qs, Ps, Rs, acc);
-            if (r >= n - kHalo) gather_row<B, SB>(r + kHalo - n, lb, off, cn, Qs, Ps, Rs, acc);
+            gather_row<B, SB>(r + kHalo, r0ofs, lb, off, cn, Qs, Ps, Rs, acc);
+            if (r < kHalo) gather_row<B, SB>(r + kHalo + n, r0ofs, lb, off, cn, Qs, Ps, Rs, acc);
+            if (r >= n - kHalo) gather_row<B, SB>(r + kHalo - n, r0ofs, lb, off, cn, Qs, Ps, Rs, acc);
             store_b<B>(s + (size_t)r * SB, acc);
         }
         c0 += kChunk;
@@ -434,7 +512,18 @@ __global__ void FFT_BOUNDS(E) k_xpass_adj(Geo g, const float2 *__restrict__ G1, 
     const float rcyY = g.rcy[Y];
     const float *rcx = g.rcx;
     const size_t obase = ((size_t)grp * N1 + Y) * N0 * B;
-    for (int idx = threadIdx.x; idx < n * B; idx += blockDim.x) s[idx] = colin[(size_t)(idx / B) * N1 * B + (idx % B)];
+    // Column Y of G1: B values per x, n0 rows N1*B apart.
+    if constexpr (B >= 2) {
+        constexpr int C = B / 2;                      // 16-byte pieces per x
+        for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
+            int xq = idx / C, c = idx - xq * C;
+            cp_async<16>(s + xq * B + 2 * c, colin + (size_t)xq * N1 * B + 2 * c);
+        }
+    } else {
+        for (int xq = threadIdx.x; xq < n; xq += blockDim.x) cp_async<8>(s + xq, colin + (size_t)xq * N1);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     auto ld = [=](int xq, int b) -> float2 { return s[xq * B + b]; };
     struct Crop {
