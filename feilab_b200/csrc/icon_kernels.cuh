@@ -382,38 +382,55 @@ constexpr int kLdPs = 20;
 // padded to 16 bytes.
 __host__ __device__ inline int lb_ld(int n1) { return (n1 + 2 * kHalo + 1 + 7) & ~7; }
 
-// Shared-memory bytes of k_ypass_adj: the rotated row (padded stride), one
-// chunk of staged entries (f values, phix*phiy window, iy0) and the row's
-// lower-bound table.
+// Shared-memory layout of k_ypass_adj.  Two chunk buffers of staged entries
+// (f values, phix*phiy window, iy0) and the row's lower-bound table are live
+// while the rows are gathered into registers; the rotated row (padded
+// stride) is written after the last chunk and shares the same bytes.
+__host__ __device__ inline size_t ypass_adj_chunk_bytes(int B)
+{
+    size_t sb = (B == 8) ? 10 : (B == 4) ? 6 : B;
+    return (size_t)kChunk * (sb * sizeof(float2) + kLdPs * sizeof(float) + sizeof(int));
+}
 __host__ __device__ inline size_t ypass_adj_smem(int n1, int B)
 {
     size_t sb = (B == 8) ? 10 : (B == 4) ? 6 : B;
-    return (size_t)n1 * sb * sizeof(float2) +
-           (size_t)kChunk * (sb * sizeof(float2) + kLdPs * sizeof(float) + sizeof(int)) +
-           (((size_t)lb_ld(n1) * sizeof(unsigned short) + 15) & ~(size_t)15);
+    size_t row = (size_t)n1 * sb * sizeof(float2);
+    size_t gather = 2 * ypass_adj_chunk_bytes(B) + (((size_t)lb_ld(n1) * sizeof(unsigned short) + 15) & ~(size_t)15);
+    return row > gather ? row : gather;
 }
 
-// Adds the staged entries with r0 in [i - 13, i] to acc: entry e puts
-// (phix * phiy)_e[i - r0_e] * f_e on buffer row i (Rs holds iy0).  lb holds the row's
-// lower-bound table, off the index of the chunk's first entry in the row.
-template <int B, int SB>
-__device__ __forceinline__ void gather_row(int i, int r0ofs, const unsigned short *lb, int off, int cn,
-                                           const float2 *Qs, const float *Ps, const int *Rs, float2 (&acc)[B])
+// Adds the staged entries covering buffer rows i0 .. i0+R-1 (r0 in
+// [i0 - 13, i0 + R - 1]) to acc[k] of row i0 + k: entry e puts
+// (phix * phiy)_e[i0 + k - r0_e] * f_e on row i0 + k when that tap is in
+// 0..13.  Rs holds iy0 (r0 = iy0 + r0ofs); lb is the row's lower-bound
+// table (last index lbmax) and off the index of the chunk's first entry.
+template <int B, int SB, int R>
+__device__ __forceinline__ void gather_rows(int i0, int r0ofs, const unsigned short *lb, int lbmax, int off, int cn,
+                                            const float2 *Qs, const float *Ps, const int *Rs, float2 (&acc)[R][B])
 {
-    int lo = min(max((int)lb[max(i - (kTaps - 1), 0)] - off, 0), cn);
-    int hi = min(max((int)lb[i + 1] - off, 0), cn);
-    const int iu = i - r0ofs;
+    // lb[lbmax] counts every entry of the row, so clamping an index past it
+    // (alias ranges of wide thread strips) is exact.
+    int lo = min(max((int)lb[min(max(i0 - (kTaps - 1), 0), lbmax)] - off, 0), cn);
+    int hi = min(max((int)lb[min(max(i0 + R, 0), lbmax)] - off, 0), cn);
+    const int iu = i0 - r0ofs;
     for (int e = lo; e < hi; ++e) {
-        float p = Ps[e * kLdPs + (iu - Rs[e])];   // i - r0 in 0..13, r0 = iy0 + r0ofs
+        const int t0 = iu - Rs[e];        // tap of row i0; row i0 + k uses t0 + k
+        const float *pe = Ps + e * kLdPs;
+        float p[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k) p[k] = ((unsigned)(t0 + k) < (unsigned)kTaps) ? pe[t0 + k] : 0.f;
         float2 q[B];
         load_b<B>(Qs + e * SB, q);
 #pragma unroll
-        for (int b = 0; b < B; ++b) {
-            acc[b].x = fmaf(q[b].x, p, acc[b].x);
-            acc[b].y = fmaf(q[b].y, p, acc[b].y);
-        }
+        for (int k = 0; k < R; ++k)
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                acc[k][b].x = fmaf(q[b].x, p[k], acc[k][b].x);
+                acc[k][b].y = fmaf(q[b].y, p[k], acc[k][b].y);
+            }
     }
 }
+
 
 // -------------------------------------------------------------- K2T ----
 // Adjoint y-pass.  Entry e (node j, x tap t0) of row x adds
@@ -424,10 +441,10 @@ __device__ __forceinline__ void gather_row(int i, int r0ofs, const unsigned shor
 // contiguous range r0 in [i - 13, i], read from the precomputed lower-bound
 // table.  The 8 halo rows on each side alias rows n-8..n-1 and 0..7, so
 // those rows also gather the range of their alias.  Entries are copied in
-// chunks with cp.async (f_j, the phix*phiy window, iy0); a row's partial sum
-// stays in its own buffer row between chunks, so only the staging needs
-// barriers and every row gets its terms in a fixed order, with no atomics.
-// Then the inverse FFT
+// chunks with cp.async (f_j, the phix*phiy window, iy0), the next chunk in
+// flight while the current one is gathered; a thread keeps its rows' sums in
+// registers across chunks, so every row gets its terms in a fixed order, with
+// no atomics.  The sums then go to the rotated row buffer and the inverse FFT
 // along y (NU:1203) reads the rotated row, and its last pass writes the rows
 // Y < N1 of the crop (NU:1104-1121: y = (Y + n1 - N1/2) % n1) straight to
 // G1[x][Y][b].  blockDim.x is max(32, n1*B/E); GUARD when that is more than
@@ -437,20 +454,25 @@ __global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, f
 {
     extern __shared__ float2 s[];
     constexpr int SB = RowStride<B>::v;
+    constexpr int R = E / B;               // rows per thread: thread t owns rows t + k*T, k < R
     const int grp = blockIdx.x, x = blockIdx.y, n = g.n1, N1 = g.N1;
-    float2 *Qs = s + (size_t)n * SB;                           // [kChunk][SB]
-    float *Ps = reinterpret_cast<float *>(Qs + kChunk * SB);   // [kChunk][kLdPs]
-    int *Rs = reinterpret_cast<int *>(Ps + kChunk * kLdPs);    // [kChunk]
-    unsigned short *lb = reinterpret_cast<unsigned short *>(Rs + kChunk);
-    const int e0 = g.row_off[x], e1 = g.row_off[x + 1];
+    char *const base = reinterpret_cast<char *>(s);
+    const size_t cbytes = ypass_adj_chunk_bytes(B);
+    unsigned short *lb = reinterpret_cast<unsigned short *>(base + 2 * cbytes);
+    const int e0 = g.row_off[x], cnt = g.row_off[x + 1] - e0;
     const float2 *fg = f + (size_t)grp * g.M * B;
     const int T = blockDim.x, ldl = lb_ld(n);
     const int r0ofs = n / 2 + kHalo;
-    copy_async(lb, g.ent_lb + (size_t)x * ldl, (size_t)ldl * sizeof(unsigned short));   // waited for with chunk 0
-    int c0 = e0;
-    do {
-        const int cn = min(kChunk, e1 - c0);
-        __syncthreads();
+    const int nch = (cnt + kChunk - 1) / kChunk;
+    // Chunk c lives in buffer c & 1: Qs [kChunk][SB], Ps [kChunk][kLdPs], Rs [kChunk].
+    auto bufQ = [&](int c) { return reinterpret_cast<float2 *>(base + (c & 1) * cbytes); };
+    auto bufP = [&](int c) { return reinterpret_cast<float *>(bufQ(c) + kChunk * SB); };
+    auto bufR = [&](int c) { return reinterpret_cast<int *>(bufP(c) + kChunk * kLdPs); };
+    auto issue = [&](int c) {
+        const int c0 = e0 + c * kChunk, cn = min(kChunk, e0 + cnt - c0);
+        float2 *Qs = bufQ(c);
+        float *Ps = bufP(c);
+        int *Rs = bufR(c);
         for (int i = threadIdx.x; i < cn; i += T) {
             const int j = __ldg(&g.ent_jt[c0 + i]) >> 4;
             const float2 *src = fg + (size_t)j * B;
@@ -466,24 +488,41 @@ __global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, f
             cp_async<4>(Rs + i, g.ent_iy0 + c0 + i);
         }
         cp_async_commit();
-        cp_async_wait<0>();
-        __syncthreads();
-        const int off = c0 - e0;
-        for (int r = threadIdx.x; r < n; r += T) {
-            float2 acc[B];
-            if (off == 0) {
+    };
+    float2 acc[R][1][B];                  // gather_rows<..., 1> takes one row as [1][B]
 #pragma unroll
-                for (int b = 0; b < B; ++b) acc[b] = make_float2(0.f, 0.f);
-            } else {
-                load_b<B>(s + (size_t)r * SB, acc);
+    for (int k = 0; k < R; ++k)
+#pragma unroll
+        for (int b = 0; b < B; ++b) acc[k][0][b] = make_float2(0.f, 0.f);
+    if (nch > 0) {
+        copy_async(lb, g.ent_lb + (size_t)x * ldl, (size_t)ldl * sizeof(unsigned short));
+        issue(0);
+    }
+    for (int c = 0; c < nch; ++c) {
+        cp_async_wait<0>();
+        __syncthreads();                  // chunk c landed; chunk c-1's buffer is free
+        if (c + 1 < nch) issue(c + 1);
+        const int off = c * kChunk, cn = min(kChunk, cnt - off);
+        const float2 *Qs = bufQ(c);
+        const float *Ps = bufP(c);
+        const int *Rs = bufR(c);
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const int r = threadIdx.x + k * T;
+            if (r < n) {
+                gather_rows<B, SB, 1>(r + kHalo, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
+                // Rows 0..7 and n-8..n-1 also take the halo rows that alias them.
+                if (r < kHalo) gather_rows<B, SB, 1>(r + kHalo + n, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
+                if (r >= n - kHalo) gather_rows<B, SB, 1>(r + kHalo - n, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
             }
-            gather_row<B, SB>(r + kHalo, r0ofs, lb, off, cn, Qs, Ps, Rs, acc);
-            if (r < kHalo) gather_row<B, SB>(r + kHalo + n, r0ofs, lb, off, cn, Qs, Ps, Rs, acc);
-            if (r >= n - kHalo) gather_row<B, SB>(r + kHalo - n, r0ofs, lb, off, cn, Qs, Ps, Rs, acc);
-            store_b<B>(s + (size_t)r * SB, acc);
         }
-        c0 += kChunk;
-    } while (c0 < e1);
+    }
+    __syncthreads();                      // the row buffer reuses the chunk buffers
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int r = threadIdx.x + k * T;
+        if (r < n) store_b<B>(s + (size_t)r * SB, acc[k][0]);
+    }
     __syncthreads();
     float2 *row = s;
     float2 *out = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
