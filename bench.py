@@ -177,7 +177,7 @@ def run_reference(args):
 def run_ours(args):
     import torch
     import torch.distributed as dist
-    from feilab_b200 import icon
+    from feilab_b200 import icon, sharding
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -191,7 +191,7 @@ def run_ours(args):
     S = SLICES_PER_STEP
     nsteps = args.warmup + args.steps
     # This rank's slices: disjoint y ranges per rank (weak scaling).
-    ys = [(rank * nsteps * S + i) % NY for i in range(nsteps * S)]
+    ys = sharding.rank_slices(rank, world, nsteps, S, NY)
     rows, tilts = make_rows(ys, dev)
     rows = rows.view(nsteps, S, len(tilts), NX).contiguous()
     plan = icon.IconPlan(NX, THICK, tilts, capacity=S, device=local)
@@ -203,11 +203,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return sharding.max_over_ranks(x, world, device=dev)
 
     # ---- device-resident inputs (value) -------------------------------------
     for i in range(args.warmup):
@@ -236,7 +232,7 @@ def run_ours(args):
     plan.trace(False)
     t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     clocks = clk.summary()
-    value = world * S * args.steps / t_dev
+    value = sharding.job_rate(world, S, args.steps, t_dev)
 
     # ---- end to end: host rows in, host slices out ------------------------
     h_rows = torch.empty((nsteps, S, len(tilts), NX), dtype=torch.float32, pin_memory=True)
@@ -252,7 +248,7 @@ def run_ours(args):
     e1.record(stream)
     barrier()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-    e2e = world * S * args.steps / t_e2e
+    e2e = sharding.job_rate(world, S, args.steps, t_e2e)
 
     # ---- roofline of the dominant kernel ----------------------------------
     peak, peak_kind = measured_peaks()
