@@ -22,9 +22,11 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.pa
 
 # (source, extra flags, object): the batched FFT kernels are built once per
 # slice-group size B, in parallel.
-LIB_UNITS = [("icon_api.cu", [], "icon_api.o"), ("icon_noalloc.cu", [], "icon_noalloc.o")] + [
+LIB_UNITS = [("icon_api.cu", [], "icon_api.o"), ("icon_noalloc.cu", [], "icon_noalloc.o"),
+             ("ws_api.cu", [], "ws_api.o")] + [
     ("icon_kern_b.cu", ["-DICON_KB=%d" % b], "icon_kern_b%d.o" % b) for b in (1, 2, 4, 8)]
-LIB_DEPS = ["icon_api.cu", "icon_noalloc.cu", "icon_kern_b.cu", "icon_launch.h", "icon_kernels.cuh", "icon_device.cuh"]
+LIB_DEPS = ["icon_api.cu", "icon_noalloc.cu", "icon_kern_b.cu", "icon_launch.h", "icon_kernels.cuh", "icon_device.cuh",
+            "ws_api.cu", "ws_conv.cuh", "ws_tc.cuh"]
 BUILD_DIR = os.path.join(HERE, "_build")
 CLI_SOURCES = ["icon_cli.cpp", "mrc_io.cpp"]
 
@@ -44,7 +46,8 @@ def _nvcc():
 
 
 def build_lib(force=False, verbose=False):
-    deps = [os.path.join(CSRC, f) for f in LIB_DEPS] + [os.path.join(ROOT, "include", "icon_b200.h")]
+    deps = [os.path.join(CSRC, f) for f in LIB_DEPS] + [os.path.join(ROOT, "include", h)
+                                                        for h in ("icon_b200.h", "icon_warmstart.h")]
     if not force and not _stale(LIB, deps):
         return LIB
     os.makedirs(BUILD_DIR, exist_ok=True)

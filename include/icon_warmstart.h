@@ -1,0 +1,51 @@
+/* icon_warmstart.h -- learned warm start for the ICON solve.
+ *
+ * The reference (ICON-GPU v1.2.9) starts every solve from m = 0
+ * (cudaMemset of m before the loop, IG/Iteration2.cu:33).  This library adds
+ * a start predicted by a small U-Net from the slice's back-projection
+ * Re(A^H W b): 4 levels of 16/32/64/128 channels, 3x3 convolutions with ReLU,
+ * 2x2 average pooling, nearest upsampling and skip connections, BF16
+ * activations and weights with FP32 accumulation on the sm_100a tensor cores
+ * (tcgen05.mma fed by TMA).  None of this has a reference counterpart; the
+ * solve that follows is the reference's algorithm unchanged (icon_solve with
+ * warm_start = 1).
+ *
+ * All device pointers are caller-owned; stream arguments are cudaStream_t
+ * passed as void *.  Functions return icon_status (icon_b200.h) and leave a
+ * message for icon_last_error() on failure.
+ */
+#ifndef ICON_WARMSTART_H
+#define ICON_WARMSTART_H
+
+#include <stddef.h>
+
+#include "icon_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One 3x3 convolution (stride 1, zero padding 1) on the tensor cores, the
+ * building block of the network, exported for tests and other callers.
+ * in0 [nimg][H][W][cin0] and, when in1 is not NULL, in1 [nimg][H][W][cin1]
+ * are BF16 NHWC tensors read as one input of cin0 + cin1 channels (each a
+ * multiple of 16).  w: BF16 [9][N][cin0 + cin1] with tap = 3*dy + dx;
+ * bias: FP32 [N] or NULL; relu: 0 or 1.  Output channels [0, nsplit) go to
+ * out0 [nimg][H][W][nsplit] and [nsplit, N) to out1 [nimg][H][W][N - nsplit];
+ * acc0 / acc1 = 1 add to the output's values instead of overwriting them.
+ * N and nsplit are multiples of 16, N <= 256. */
+icon_status icon_ws_conv3x3(const void *in0, int cin0, const void *in1, int cin1, int nimg, int H, int W,
+                            const void *w, const float *bias, int N, int relu, void *out0, int nsplit, int acc0,
+                            void *out1, int acc1, void *stream);
+
+/* Reads and clears the current device's error flag of the tensor-core
+ * kernels (0: none; 1, 2, 3: a bounded wait for a TMA load, for the MMAs of
+ * a stage, or for the accumulator ran out; the kernel then skipped its
+ * output).  Synchronises with the device. */
+icon_status icon_ws_device_error(int *h_code);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ICON_WARMSTART_H */
