@@ -24,6 +24,24 @@ def lib():
         L.icon_ws_conv3x3.restype = ctypes.c_int
         L.icon_ws_device_error.argtypes = [ctypes.POINTER(I)]
         L.icon_ws_device_error.restype = ctypes.c_int
+        F, D, Z = ctypes.c_float, ctypes.c_double, ctypes.c_size_t
+        L.icon_ws_create.argtypes = [P, I, ctypes.POINTER(P)]
+        L.icon_ws_destroy.argtypes = [P]
+        L.icon_ws_param_count.argtypes = []
+        L.icon_ws_param_count.restype = Z
+        L.icon_ws_init.argtypes = [P, ctypes.c_ulonglong]
+        L.icon_ws_set_params.argtypes = [P, V, Z, F]
+        L.icon_ws_get_params.argtypes = [P, V, Z, ctypes.POINTER(F)]
+        L.icon_ws_set_gain.argtypes = [P, F]
+        L.icon_ws_predict.argtypes = [P, V, V, I, V]
+        L.icon_ws_backprop.argtypes = [P, V, V, I, ctypes.POINTER(D), V]
+        L.icon_ws_get_grads.argtypes = [P, V, Z]
+        L.icon_ws_update.argtypes = [P, F, V]
+        L.icon_ws_train_step.argtypes = [P, V, V, I, F, ctypes.POINTER(D), V]
+        for name in ("icon_ws_create", "icon_ws_destroy", "icon_ws_init", "icon_ws_set_params", "icon_ws_get_params",
+                     "icon_ws_set_gain", "icon_ws_predict", "icon_ws_backprop", "icon_ws_get_grads", "icon_ws_update",
+                     "icon_ws_train_step"):
+            getattr(L, name).restype = ctypes.c_int
         _ws_ready = True
     return L
 
@@ -65,3 +83,92 @@ def conv3x3(in0, w, bias=None, relu=False, in1=None, nsplit=None, out0=None, out
     _check(lib().icon_ws_conv3x3(_ptr(in0), c0, _ptr(in1), c1, n, H, W, _ptr(w), _ptr(bias), N, int(relu),
                                  _ptr(out0), nsplit, int(acc0), _ptr(out1), int(acc1), _stream()))
     return (out0, out1) if nsplit < N else out0
+
+
+def param_count() -> int:
+    return int(lib().icon_ws_param_count())
+
+
+class Network:
+    """The warm-start U-Net for the geometry of an IconPlan.
+
+    Slices use the plan's layout: Ahwb (S, N0, N1) complex64 as returned by
+    IconPlan.prepare_rhs, m (S, N0, N1) float32 as IconPlan.solve takes and
+    returns.  predict() gives the start to pass as IconPlan.solve(m0=...)."""
+
+    def __init__(self, plan, capacity=None):
+        import torch
+        self.plan = plan
+        self.capacity = int(capacity or plan.capacity)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(plan.device):
+            _check(lib().icon_ws_create(plan._h, self.capacity, ctypes.byref(h)))
+        self._h = h
+        self.n = param_count()
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().icon_ws_destroy(h)
+            self._h = None
+
+    __del__ = close
+
+    def init(self, seed=0):
+        _check(lib().icon_ws_init(self._h, ctypes.c_ulonglong(int(seed))))
+
+    def set_params(self, params, gain=1.0):
+        import numpy as np
+        p = np.ascontiguousarray(np.asarray(params, np.float32))
+        if p.size != self.n:
+            raise IconError(f"expected {self.n} parameters, got {p.size}")
+        _check(lib().icon_ws_set_params(self._h, p.ctypes.data_as(ctypes.c_void_p), self.n, float(gain)))
+
+    def get_params(self):
+        import numpy as np
+        p = np.zeros(self.n, np.float32)
+        g = ctypes.c_float(0)
+        _check(lib().icon_ws_get_params(self._h, p.ctypes.data_as(ctypes.c_void_p), self.n, ctypes.byref(g)))
+        return p, float(g.value)
+
+    def set_gain(self, gain):
+        _check(lib().icon_ws_set_gain(self._h, float(gain)))
+
+    def grads(self):
+        import numpy as np
+        p = np.zeros(self.n, np.float32)
+        _check(lib().icon_ws_get_grads(self._h, p.ctypes.data_as(ctypes.c_void_p), self.n))
+        return p
+
+    def _in(self, Ahwb, m=None):
+        import torch
+        P = self.plan
+        if Ahwb.dtype != torch.complex64 or not Ahwb.is_contiguous() or Ahwb.shape[1:] != (P.N0, P.N1):
+            raise IconError("Ahwb must be a contiguous (S, N0, N1) complex64 tensor")
+        if m is not None and (m.dtype != torch.float32 or not m.is_contiguous() or m.shape != Ahwb.shape):
+            raise IconError("target must be a contiguous (S, N0, N1) float32 tensor")
+        return Ahwb.shape[0]
+
+    def predict(self, Ahwb, out=None):
+        import torch
+        S = self._in(Ahwb)
+        if out is None:
+            out = torch.empty((S, self.plan.N0, self.plan.N1), dtype=torch.float32, device=Ahwb.device)
+        _check(lib().icon_ws_predict(self._h, _ptr(Ahwb), _ptr(out), S, _stream()))
+        return out
+
+    def backprop(self, Ahwb, target):
+        S = self._in(Ahwb, target)
+        loss = ctypes.c_double(0)
+        _check(lib().icon_ws_backprop(self._h, _ptr(Ahwb), _ptr(target), S, ctypes.byref(loss), _stream()))
+        return float(loss.value)
+
+    def update(self, lr):
+        _check(lib().icon_ws_update(self._h, float(lr), _stream()))
+
+    def train_step(self, Ahwb, target, lr):
+        S = self._in(Ahwb, target)
+        loss = ctypes.c_double(0)
+        _check(lib().icon_ws_train_step(self._h, _ptr(Ahwb), _ptr(target), S, float(lr), ctypes.byref(loss),
+                                        _stream()))
+        return float(loss.value)

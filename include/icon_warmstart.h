@@ -38,6 +38,50 @@ icon_status icon_ws_conv3x3(const void *in0, int cin0, const void *in1, int cin1
                             const void *w, const float *bias, int N, int relu, void *out0, int nsplit, int acc0,
                             void *out1, int acc1, void *stream);
 
+/* The network.  Slices are in the layout of icon_prepare_rhs / icon_solve:
+ * Ahwb [S][N0][N1] complex (pairs of float), m [S][N0][N1] float, Y
+ * fastest.  The network image of a slice is Re(Ahwb) as N1 rows of N0
+ * pixels, padded to multiples of 8 and divided by its RMS; its output times
+ * the same RMS and a fixed gain is the predicted start.  Parameters are FP32
+ * masters (BF16 copies feed the tensor cores); training uses Adam (beta
+ * 0.9 / 0.999, eps 1e-8) on the mean squared error over the valid pixels in
+ * network units. */
+typedef struct icon_ws icon_ws;
+
+/* Network for the geometry (N0, N1) of `plan`, on the current device, for
+ * up to `capacity` slices per call (at most the plan's capacity). */
+icon_status icon_ws_create(icon_plan *plan, int capacity, icon_ws **out);
+icon_status icon_ws_destroy(icon_ws *ws);
+
+/* Number of FP32 parameters. */
+size_t icon_ws_param_count(void);
+
+/* He-normal initialisation from a seed; resets the optimiser. */
+icon_status icon_ws_init(icon_ws *ws, unsigned long long seed);
+
+/* Copies all parameters and the output gain (> 0) in or out. */
+icon_status icon_ws_set_params(icon_ws *ws, const float *h_params, size_t count, float gain);
+icon_status icon_ws_get_params(icon_ws *ws, float *h_params, size_t count, float *h_gain);
+icon_status icon_ws_set_gain(icon_ws *ws, float gain);
+
+/* m0 [S][N0][N1] = network(Ahwb): the warm start for icon_solve. */
+icon_status icon_ws_predict(icon_ws *ws, const void *d_Ahwb, float *d_m0, int S, void *stream);
+
+/* Forward pass, mean squared error against d_target [S][N0][N1] (both in
+ * network units: divided by RMS * gain), and the gradients of every
+ * parameter, kept in the network (icon_ws_get_grads copies them out).
+ * *h_loss (optional; synchronises) receives the loss. */
+icon_status icon_ws_backprop(icon_ws *ws, const void *d_Ahwb, const float *d_target, int S, double *h_loss,
+                             void *stream);
+icon_status icon_ws_get_grads(icon_ws *ws, float *h_grads, size_t count);
+
+/* One Adam step with learning rate lr from the last gradients. */
+icon_status icon_ws_update(icon_ws *ws, float lr, void *stream);
+
+/* icon_ws_backprop followed by icon_ws_update. */
+icon_status icon_ws_train_step(icon_ws *ws, const void *d_Ahwb, const float *d_target, int S, float lr,
+                               double *h_loss, void *stream);
+
 /* Reads and clears the current device's error flag of the tensor-core
  * kernels (0: none; 1, 2, 3: a bounded wait for a TMA load, for the MMAs of
  * a stage, or for the accumulator ran out; the kernel then skipped its
