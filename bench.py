@@ -287,6 +287,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": int(S * NX * THICK * 4)},
             "gpu_launches": int(launches),
             "clocks": clocks}
+    line["warm_start"] = warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S)
     if rank == 0 and world == 1 and not args.no_cpu:
         ncpu = os.cpu_count() or 1
         rows_cpu = rows.view(-1, len(tilts), NX)[:ncpu].cpu().numpy()
@@ -299,6 +300,60 @@ def run_ours(args):
     plan.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S):
+    """The learned warm start against the plain solve on the same slices:
+    timed input stage + network + full schedule (device-resident inputs),
+    the FRC of its result against the plain result (the judge), and the
+    held-out iterations-to-tolerance comparison stored with the weights."""
+    import torch
+    from feilab_b200 import sharding, warmstart
+    from feilab_b200.train_warmstart import frc_mean
+    try:
+        params, gain, meta = warmstart.load_weights(nx=NX, thickness=THICK)
+    except OSError as e:
+        return {"unavailable": f"no trained weights: {e}"}
+    cap = 32
+    net = warmstart.Network(plan, capacity=cap)
+    net.set_params(params, gain)
+
+    def step(i):
+        A = plan.prepare_rhs(rows[i])
+        m0 = torch.empty((S, NX, THICK), dtype=torch.float32, device=A.device)
+        for s0 in range(0, S, cap):
+            net.predict(A[s0:s0 + cap], out=m0[s0:s0 + cap])
+        return A, m0, plan.solve(A, SCHED, DATA_TYPE, THRESHOLD, m0=m0)
+
+    for i in range(args.warmup):
+        step(i)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.warmup, args.warmup + args.steps):
+        A, m0, m_warm = step(i)
+    e1.record(stream)
+    barrier()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    # inference alone, and the judge: FRC of the warm result against the cold one
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for s0 in range(0, S, cap):
+        net.predict(A[s0:s0 + cap], out=m0[s0:s0 + cap])
+    f1.record(stream)
+    m_cold = plan.solve(A, SCHED, DATA_TYPE, THRESHOLD)
+    torch.cuda.synchronize()
+    frc = frc_mean(m_warm[:16], m_cold[:16])
+    net.close()
+    return {"value": sharding.job_rate(world, S, args.steps, t), "unit": "slices/s",
+            "schedule": "network start + the full reference schedule", "inference_ms_per_slice":
+            round(f0.elapsed_time(f1) / S, 4), "frc_vs_cold_min": round(float(frc.min()), 4),
+            "heldout_icon_iterations_to_frc_0.99": {"cold": meta.get("icon_iters_to_frc099_cold"),
+                                                    "warm": meta.get("icon_iters_to_frc099_warm")},
+            "heldout_prediction_frc_min": meta.get("prediction_frc_min"),
+            "gain_to_tolerance": (round(meta["icon_iters_to_frc099_cold"] / meta["icon_iters_to_frc099_warm"], 3)
+                                  if meta.get("icon_iters_to_frc099_warm") else None),
+            "weights": f"feilab_b200/weights/warmstart_{NX}x{THICK}.npz (trained on {meta.get('train_slices')} slices)"}
 
 
 def run_profile_case(args):

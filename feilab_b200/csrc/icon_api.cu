@@ -187,6 +187,7 @@ struct icon_plan {
     float2 *G1 = nullptr, *P = nullptr, *f = nullptr, *rhat = nullptr, *Ahwb = nullptr, *imgc = nullptr;
     float *m = nullptr, *rows = nullptr, *outrp = nullptr, *mout = nullptr;
     double *part_rtr = nullptr, *part_rtar = nullptr, *alpha = nullptr;
+    double *step_part = nullptr, *step = nullptr;   // relative update size (icon_solve_until)
     int k3_blocks = 0;
     // reprojection lines, keyed by the .tlt angle
     std::map<float, std::unique_ptr<NodeTables>> lines;
@@ -458,7 +459,7 @@ icon_status launch_rows(icon_plan *p, const float *d_rows, int S, int G, float2 
 
 // One ICON iteration over G groups (Iteration2.cu:53-132 with Alpha2).
 icon_status launch_iteration(icon_plan *p, int G, bool clamp, int data_type, float thr, double *hist_a, double *hist_r,
-                             cudaStream_t st)
+                             cudaStream_t st, bool measure_step = false)
 {
     ICON_TRY(launch_forward(p, p->nodes, p->m, true, G, 1, p->f, st));          // f = W A m
     ICON_TRY(launch_adjoint(p, p->f, G, 1, p->rhat, st));                       // rhat = A^H f - Ahwb, ||rhat||^2
@@ -468,7 +469,12 @@ icon_status launch_iteration(icon_plan *p, int G, bool clamp, int data_type, flo
     int per_group = p->N1 * p->N0 * p->B;
     dim3 gu((unsigned)std::min<size_t>(((size_t)per_group + 255) / 256, 512), G);
     WITH_B(p->B, LAUNCH_B(p, K_UPD, st, stage_bytes(p, p->nodes).upd * G * p->B,
-                          L::update(gu, st, p->m, p->rhat, p->alpha, per_group, clamp ? 1 : 0, data_type, thr)))
+                          L::update(gu, st, p->m, p->rhat, p->alpha, per_group, clamp ? 1 : 0, data_type, thr,
+                                    measure_step ? p->step_part : nullptr)))
+    if (measure_step) {                                                          // ||m_new - m_old|| / ||m_new||
+        const int slots = G * p->B;
+        LAUNCH(p, K_UPD, st, icon::k_step_reduce<<<(slots + 127) / 128, 128, 0, st>>>(p->step_part, (int)gu.x, p->B, slots, p->step));
+    }
     ICON_CUDA(cudaGetLastError());
     return ICON_OK;
 }
@@ -652,6 +658,8 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
     ICON_TRY(p->arena.alloc(&p->part_rtr, G * p->N1 * Bz));
     ICON_TRY(p->arena.alloc(&p->part_rtar, G * p->k3_blocks * Bz));
     ICON_TRY(p->arena.alloc(&p->alpha, G * Bz));
+    ICON_TRY(p->arena.alloc(&p->step_part, G * 512 * Bz * 2));
+    ICON_TRY(p->arena.alloc(&p->step, G * Bz));
     ICON_CUDA(cudaDeviceSynchronize());
     *out = p.release();
     return ICON_OK;
@@ -808,6 +816,56 @@ icon_status icon_solve(icon_plan *p, const icon_solve_cfg *cfg, const void *d_Ah
                     if (h_rtr) h_rtr[(size_t)it * S + s] = hv[(size_t)(iters + it) * slots + s];
                 }
     }
+    return rc;
+}
+
+icon_status icon_solve_until(icon_plan *p, const icon_solve_cfg *cfg, const void *d_Ahwb, float *d_m, int S,
+                            int warm_start, double tol, int check_every, int *h_iters, double *h_step, void *stream)
+{
+    ICON_TRY(check_plan(p, S));
+    if (!cfg || !d_Ahwb || !d_m) return fail(ICON_ERR_INVALID, "null argument");
+    if (!(tol >= 0.0) || check_every < 1) return fail(ICON_ERR_INVALID, "tol must be >= 0 and check_every >= 1");
+    const int a = cfg->infr_before, b = cfg->icon, c = cfg->infr_after;
+    if (a < 0 || b < 0 || c < 0) return fail(ICON_ERR_INVALID, "negative iteration count");
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int G = groups(p, S);
+    const size_t tot = (size_t)G * p->N1 * p->N0 * p->B, slots = (size_t)G * p->B;
+    LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float2><<<grid1d(tot), 256, 0, st>>>((const float2 *)d_Ahwb, p->Ahwb, S, p->N0, p->N1, p->B, tot));
+    if (warm_start) LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float><<<grid1d(tot), 256, 0, st>>>(d_m, p->m, S, p->N0, p->N1, p->B, tot));
+    else ICON_CUDA(cudaMemsetAsync(p->m, 0, tot * sizeof(float), st));
+    std::vector<double> hs(slots);
+    icon_status rc = ICON_OK;
+    int done = 0;
+    auto run = [&](int n, bool clamp, bool checked) {
+        for (int k = 0; k < n && rc == ICON_OK; ++k) {
+            const bool check = checked && ((k + 1) % check_every == 0 || k + 1 == n);
+            rc = launch_iteration(p, G, clamp, cfg->data_type, cfg->threshold, nullptr, nullptr, st, check);
+            ++done;
+            if (rc != ICON_OK || !check) continue;
+            cudaError_t e = cudaMemcpyAsync(hs.data(), p->step, sizeof(double) * slots, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) {
+                rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+                break;
+            }
+            bool all = true;
+            for (int s = 0; s < S; ++s) {
+                if (h_step) h_step[s] = hs[s];
+                if (!(hs[s] <= tol)) all = false;
+            }
+            if (all) break;
+        }
+    };
+    run(a, false, false);   // INFR (Iteration2.cu:129-132)
+    run(b, true, true);     // ICON, stopped once every slice's step is within tol
+    run(c, false, false);   // INFR
+    if (rc == ICON_OK) {
+        LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float><<<grid1d((size_t)S * p->N0 * p->N1), 256, 0, st>>>(p->m, d_m, S, p->N0, p->N1, p->B));
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (h_iters) *h_iters = done;
     return rc;
 }
 

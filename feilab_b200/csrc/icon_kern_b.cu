@@ -82,9 +82,10 @@ void Launch<B>::row_adj(int E, dim3 grid, int threads, size_t smem, cudaStream_t
 
 template <int B>
 void Launch<B>::update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat, const double *alpha, int per_group,
-                       int clamp, int data_type, float thr)
+                       int clamp, int data_type, float thr, double *step_part)
 {
-    k_update<B><<<grid, 256, 0, st>>>(m, rhat, alpha, per_group, clamp, data_type, thr);
+    if (step_part) k_update<B, true><<<grid, 256, 0, st>>>(m, rhat, alpha, per_group, clamp, data_type, thr, step_part);
+    else k_update<B, false><<<grid, 256, 0, st>>>(m, rhat, alpha, per_group, clamp, data_type, thr);
 }
 
 template <int B>

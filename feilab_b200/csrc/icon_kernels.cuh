@@ -772,21 +772,40 @@ __global__ void k_alpha(const double *__restrict__ part_rtr, int nr, const doubl
     }
 }
 
+// Relative step of the last measured update per slot:
+// out[slot] = sqrt(sum (m_new - m_old)^2 / sum m_new^2) over the blocks'
+// partial sums step_part[grp][nb][B][2] (fixed order); 0 when m_new = 0.
+__global__ void k_step_reduce(const double *__restrict__ step_part, int nb, int B, int slots, double *__restrict__ out)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= slots) return;
+    const int grp = s / B, b = s % B;
+    double d = 0.0, n = 0.0;
+    for (int k = 0; k < nb; ++k) {
+        const double *p = step_part + (((size_t)grp * nb + k) * B + b) * 2;
+        d += p[0];
+        n += p[1];
+    }
+    out[s] = n > 0.0 ? sqrt(d / n) : 0.0;
+}
+
 #endif  // ICON_KERNELS_TEMPLATES_ONLY
 
 // m <- m - alpha*Re(rhat) computed in double and stored as float; ICON steps
 // also clamp (ICONUpdateCU_R NU:1597-1616, INFRUpdateCU_R NU:1630-1639).
 // m: [G][N1][N0][B] float, rhat: same layout float2.  blockIdx.y = group.
-template <int B>
+template <int B, bool MEASURE = false>
 __global__ void k_update(float *__restrict__ m, const float2 *__restrict__ rhat, const double *__restrict__ alpha,
-                         int per_group, int clamp, int data_type, float thr)
+                         int per_group, int clamp, int data_type, float thr, double *__restrict__ step_part = nullptr)
 {
     const int grp = blockIdx.y;
     float *mg = m + (size_t)grp * per_group;
     const float2 *rg = rhat + (size_t)grp * per_group;
+    double dd = 0.0, mm = 0.0;   // MEASURE: sums of (m_new - m_old)^2 and m_new^2 of this thread's slot
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < per_group; i += gridDim.x * blockDim.x) {
         double a = alpha[grp * B + (i & (B - 1))];
-        float v = (float)((double)mg[i] - a * (double)rg[i].x);
+        const float old = mg[i];
+        float v = (float)((double)old - a * (double)rg[i].x);
         if (clamp) {
             if (data_type == 1) {
                 if (v > thr) v = thr;
@@ -795,6 +814,30 @@ __global__ void k_update(float *__restrict__ m, const float2 *__restrict__ rhat,
             }
         }
         mg[i] = v;
+        if (MEASURE) {
+            const double d = (double)v - (double)old;
+            dd += d * d;
+            mm += (double)v * (double)v;
+        }
+    }
+    if (MEASURE) {
+        // The grid stride is a multiple of B, so thread t always updates slot
+        // t % B: sum the block's threads of each slot in a fixed order into
+        // step_part[grp][block][slot][2].
+        __shared__ double red[2][256];
+        red[0][threadIdx.x] = dd;
+        red[1][threadIdx.x] = mm;
+        __syncthreads();
+        if ((int)threadIdx.x < B) {
+            double s0 = 0.0, s1 = 0.0;
+            for (int t = threadIdx.x; t < (int)blockDim.x; t += B) {
+                s0 += red[0][t];
+                s1 += red[1][t];
+            }
+            double *o = step_part + (((size_t)grp * gridDim.x + blockIdx.x) * B + threadIdx.x) * 2;
+            o[0] = s0;
+            o[1] = s1;
+        }
     }
 }
 

@@ -25,7 +25,7 @@ struct Launch {
     static void row_adj(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const Geo1 &g1,
                         const float2 *f, float *out, int S);
     static void update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat, const double *alpha, int per_group,
-                       int clamp, int data_type, float thr);
+                       int clamp, int data_type, float thr, double *step_part = nullptr);
     // Raises the dynamic shared-memory limit of every kernel variant a plan uses.
     static cudaError_t set_smem(int ex, int ey, size_t smem_x, size_t need_x, size_t smem_y, size_t smem_ya);
 };

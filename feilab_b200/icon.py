@@ -43,6 +43,8 @@ def lib():
         L.icon_rows_forward.argtypes = [P, V, V, I, V]
         L.icon_prepare_rhs.argtypes = [P, V, V, I, V]
         L.icon_solve.argtypes = [P, ctypes.POINTER(SolveCfg), V, V, I, I, V, V, V]
+        L.icon_solve_until.argtypes = [P, ctypes.POINTER(SolveCfg), V, V, I, I, ctypes.c_double, I,
+                                       ctypes.POINTER(I), V, V]
         L.icon_reproject.argtypes = [P, V, F, V, I, V]
         L.icon_reconstruct_host.argtypes = [P, ctypes.POINTER(SolveCfg), V, V, V, I, V]
         L.icon_trace_enable.argtypes = [P, I]
@@ -52,7 +54,7 @@ def lib():
         L.icon_last_error.restype = ctypes.c_char_p
         for name in ("icon_plan_create", "icon_plan_destroy", "icon_plan_query", "icon_plan_geometry",
                      "icon_nufft_forward", "icon_nufft_forward_complex", "icon_nufft_adjoint",
-                     "icon_rows_forward", "icon_prepare_rhs", "icon_solve", "icon_reproject",
+                     "icon_rows_forward", "icon_prepare_rhs", "icon_solve", "icon_solve_until", "icon_reproject",
                      "icon_reconstruct_host", "icon_trace_enable", "icon_trace_read"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
@@ -182,6 +184,28 @@ class IconPlan:
         if history:
             return m, ha[:n], hr[:n]
         return m
+
+    def solve_until(self, Ahwb, tol=0.0, iters=(0, 10, 0), data_type=1, threshold=0.03, m0=None, check_every=10):
+        """Iteration3 whose ICON phase ends once every slice's relative step
+        ||m_new - m_old|| / ||m_new|| is at or below tol (checked every
+        check_every ICON iterations).  Returns (m, iterations done, relative
+        step per slice at the last check)."""
+        import torch
+        S = Ahwb.shape[0]
+        a, b, c = iters
+        cfg = SolveCfg(int(a), int(b), int(c), int(data_type), float(threshold))
+        if m0 is None:
+            m = torch.empty((S, self.N0, self.N1), dtype=torch.float32, device=self.device)
+            warm = 0
+        else:
+            m = self._dev(m0, torch.float32).clone()
+            warm = 1
+        n = ctypes.c_int(0)
+        step = np.zeros(S, np.float64)
+        _check(lib().icon_solve_until(self._h, ctypes.byref(cfg), _ptr(self._dev(Ahwb, torch.complex64)), _ptr(m), S,
+                                      warm, float(tol), int(check_every), ctypes.byref(n),
+                                      step.ctypes.data_as(ctypes.c_void_p), _stream()))
+        return m, int(n.value), step
 
     def reproject(self, m, tilt_deg=None):
         """m (S, N0, N1) float32 -> (S, nx) float32 reprojection at tilt_deg

@@ -172,3 +172,18 @@ class Network:
         _check(lib().icon_ws_train_step(self._h, _ptr(Ahwb), _ptr(target), S, float(lr), ctypes.byref(loss),
                                         _stream()))
         return float(loss.value)
+
+
+WEIGHTS_DIR = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)),
+                                         "weights")
+
+
+def load_weights(path=None, nx=1024, thickness=300):
+    """(params, gain, meta) of a trained network file (train_warmstart's
+    output); by default the one shipped for nx x thickness."""
+    import json
+    import os
+    import numpy as np
+    path = path or os.path.join(WEIGHTS_DIR, f"warmstart_{nx}x{thickness}.npz")
+    z = np.load(path)
+    return z["params"].astype(np.float32), float(z["gain"]), json.loads(str(z["meta"]))

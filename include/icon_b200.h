@@ -128,6 +128,22 @@ icon_status icon_prepare_rhs(icon_plan *plan, const float *d_rows, void *d_Ahwb,
 icon_status icon_solve(icon_plan *plan, const icon_solve_cfg *cfg, const void *d_Ahwb, float *d_m, int S,
                        int warm_start, double *h_alpha, double *h_rtr, void *stream);
 
+/* icon_solve whose ICON phase stops at a tolerance.  The schedule is the
+ * reference's (INFR for infr_before iterations, ICON with the threshold
+ * clamp for at most `icon`, INFR for infr_after; Iteration2.cu:129-132),
+ * but every check_every ICON iterations (and at the phase's last) the size
+ * of that iteration's update relative to the new image,
+ * ||m_new - m_old|| / ||m_new|| (summed in double), is read for every slice,
+ * and the ICON phase ends once all slices are at or below tol; the final
+ * INFR iterations then run as usual.  For the clamped iteration this step,
+ * not ||rhat||, goes to zero at a fixed point.  tol = 0 runs the whole
+ * schedule (the result is icon_solve's).  *h_iters receives the iterations
+ * done and h_step[S] (optional) each slice's relative step at the last
+ * check.  Synchronises the stream at every check.  The reference has no
+ * such stop: it always runs the full count. */
+icon_status icon_solve_until(icon_plan *plan, const icon_solve_cfg *cfg, const void *d_Ahwb, float *d_m, int S,
+                             int warm_start, double tol, int check_every, int *h_iters, double *h_step, void *stream);
+
 /* Reprojection of S solved slices at one tilt angle (given as in the .tlt
  * file): forward 2-D NUFFT at the nodes of that single tilt, then the 1-D
  * adjoint NUFFT, real part (reProject_NFFT2, reProject_NFFT.cu:25-42, with

@@ -48,3 +48,12 @@ def test_plan_create_without_gpu_fails_cleanly():
         assert "status" in str(e)
     else:
         raise AssertionError("plan creation without a GPU should fail")
+
+
+def test_shipped_warm_start_weights_match_the_network():
+    # The trained warm-start network shipped with the library has exactly the
+    # parameter count of the network the library builds.
+    from feilab_b200 import warmstart
+    params, gain, meta = warmstart.load_weights()
+    assert params.size == warmstart.param_count()
+    assert gain > 0 and meta["nx"] == 1024 and meta["thickness"] == 300
