@@ -23,12 +23,14 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.pa
 # (source, extra flags, object): the batched FFT kernels are built once per
 # slice-group size B, in parallel.
 LIB_UNITS = [("icon_api.cu", [], "icon_api.o"), ("icon_noalloc.cu", [], "icon_noalloc.o"),
-             ("ws_api.cu", [], "ws_api.o"), ("ws_net.cu", [], "ws_net.o")] + [
+             ("ws_api.cu", [], "ws_api.o"), ("ws_net.cu", [], "ws_net.o"),
+             ("tools.cu", [], "tools.o")] + [
     ("icon_kern_b.cu", ["-DICON_KB=%d" % b], "icon_kern_b%d.o" % b) for b in (1, 2, 4, 8)]
 LIB_DEPS = ["icon_api.cu", "icon_noalloc.cu", "icon_kern_b.cu", "icon_launch.h", "icon_kernels.cuh", "icon_device.cuh",
-            "ws_api.cu", "ws_conv.cuh", "ws_tc.cuh", "ws_net.cu", "ws_kernels.cuh"]
+            "ws_api.cu", "ws_conv.cuh", "ws_tc.cuh", "ws_net.cu", "ws_kernels.cuh", "tools.cu"]
 BUILD_DIR = os.path.join(HERE, "_build")
-CLI_SOURCES = ["icon_cli.cpp", "mrc_io.cpp"]
+# Command-line tools: executable -> sources (host C++ over the C ABI).
+TOOLS = {"icon-gpu": ["icon_cli.cpp", "mrc_io.cpp"], "icon-preprocess": ["preprocess_cli.cpp", "mrc_io.cpp"]}
 
 
 def _stale(target, deps):
@@ -47,7 +49,7 @@ def _nvcc():
 
 def build_lib(force=False, verbose=False):
     deps = [os.path.join(CSRC, f) for f in LIB_DEPS] + [os.path.join(ROOT, "include", h)
-                                                        for h in ("icon_b200.h", "icon_warmstart.h")]
+                                                        for h in ("icon_b200.h", "icon_warmstart.h", "icon_tools.h")]
     if not force and not _stale(LIB, deps):
         return LIB
     os.makedirs(BUILD_DIR, exist_ok=True)
@@ -68,18 +70,23 @@ def build_lib(force=False, verbose=False):
 
 
 def build_cli(force=False, verbose=False):
-    srcs = [os.path.join(CSRC, f) for f in CLI_SOURCES]
-    if not all(os.path.exists(s) for s in srcs):
-        return None
-    deps = srcs + [LIB, os.path.join(CSRC, "mrc_io.h"), os.path.join(ROOT, "include", "icon_b200.h")]
-    if not force and not _stale(CLI, deps):
-        return CLI
-    cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, "-o", CLI, *srcs,
-           "-L" + HERE, "-licon_b200", "-Wl,-rpath,$ORIGIN", "-lpthread"]
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
-    return CLI
+    """The command-line tools (TOOLS), linked against the library."""
+    built = []
+    for exe, sources in TOOLS.items():
+        srcs = [os.path.join(CSRC, f) for f in sources]
+        if not all(os.path.exists(s) for s in srcs):
+            continue
+        target = os.path.join(HERE, exe)
+        deps = srcs + [LIB, os.path.join(CSRC, "mrc_io.h")] + [os.path.join(ROOT, "include", h) for h in
+                                                              ("icon_b200.h", "icon_tools.h")]
+        if force or _stale(target, deps):
+            cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, "-o", target, *srcs,
+                   "-L" + HERE, "-licon_b200", "-Wl,-rpath,$ORIGIN", "-lpthread"]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
+        built.append(target)
+    return built
 
 
 def build(force=False, verbose=False):

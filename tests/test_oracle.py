@@ -4,7 +4,7 @@ sm_100a) and against mathematics (direct NDFT, adjoint identity)."""
 import numpy as np
 import pytest
 
-from conftest import min_abs_tilt_index, rel_l2
+from conftest import load_golden, min_abs_tilt_index, rel_l2
 from oracle.oracle import OraclePlan, grid_params
 
 # The reference computes in float with cuFFT; these are relative-L2 bounds of
@@ -101,3 +101,15 @@ def test_reference_cli_fixture_consistent_with_harness(golden):
             os.unlink(path)
         assert (int(h["nx"]), int(h["ny"]), int(h["nz"]), int(h["mode"])) == (nx, th, 1, 2)
         np.testing.assert_array_equal(d[0], z["ref_m"][s].T)
+
+
+@pytest.mark.parametrize("name", ["p1", "p2"])
+def test_preprocess_oracle_matches_reference_tool(name):
+    # oracle/preprocess.py against the reference ICONPreProcess's own output.
+    import oracle.preprocess as pp
+    z = load_golden("preprocess")
+    st, tilts, th = z[name + "_stack"], z[name + "_tilts"], int(z[name + "_thickness"])
+    np.testing.assert_array_equal(pp.preprocess(st), z[name + "_mode_only"])
+    got = pp.preprocess(st, tilts, th)
+    ref = z[name + "_normalized"]
+    assert np.max(np.abs(got - ref)) <= 2e-6 * np.max(np.abs(ref))
