@@ -43,3 +43,69 @@ def preprocess(stack, tilts=None, thickness=None, out=None):
                                  t.ctypes.data_as(ctypes.c_void_p) if t is not None else None,
                                  int(thickness) if t is not None else 0, _stream()))
     return out
+
+
+def _mask_lib():
+    L = lib()
+    if not getattr(L, "_mask_ready", False):
+        P, I, V, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_float
+        L.icon_mask_radius.argtypes = [I, V, I, I, V, V, I, ctypes.POINTER(F), ctypes.POINTER(F), ctypes.POINTER(I)]
+        L.icon_mask_create.argtypes = [I, V, I, F, F, I, I, I, ctypes.POINTER(P)]
+        L.icon_mask_destroy.argtypes = [P]
+        L.icon_mask_filter.argtypes = [P, V]
+        L.icon_mask_apply.argtypes = [P, V, I, I, I, V, V]
+        L.icon_volume_crop.argtypes = [V, I, I, I, I, V, V]
+        for n in ("icon_mask_radius", "icon_mask_create", "icon_mask_destroy", "icon_mask_filter", "icon_mask_apply",
+                  "icon_volume_crop"):
+            getattr(L, n).restype = ctypes.c_int
+        L._mask_ready = True
+    return L
+
+
+def mask_radius(n, tilts, radius=None, crossv=None, fullrec=None):
+    """(rate of the FRC-0.5 radius, rate of the FRC-0.3 radius, explicit?)
+    as ICONMask3 derives them; radius None reads the FRC curves."""
+    t = np.ascontiguousarray(np.asarray(tilts, np.float32))
+    cv = np.ascontiguousarray(np.asarray(crossv, np.float32)) if crossv is not None else None
+    fr = np.ascontiguousarray(np.asarray(fullrec, np.float32)) if fullrec is not None else None
+    r05, r03, ex = ctypes.c_float(), ctypes.c_float(), ctypes.c_int()
+    _check(_mask_lib().icon_mask_radius(int(n), t.ctypes.data_as(ctypes.c_void_p), t.size,
+                                        -1 if radius is None else int(radius),
+                                        cv.ctypes.data_as(ctypes.c_void_p) if cv is not None else None,
+                                        fr.ctypes.data_as(ctypes.c_void_p) if fr is not None else None,
+                                        min(cv.size, fr.size) if cv is not None and fr is not None else 0,
+                                        ctypes.byref(r05), ctypes.byref(r03), ctypes.byref(ex)))
+    return float(r05.value), float(r03.value), bool(ex.value)
+
+
+class Mask:
+    """ICONMask3's cross-validation mask for n x n slices on the GPU."""
+
+    def __init__(self, n, tilts, rate05, rate03, explicit, gauss_width=None, capacity=16):
+        t = np.ascontiguousarray(np.asarray(tilts, np.float32))
+        h = ctypes.c_void_p()
+        _check(_mask_lib().icon_mask_create(int(n), t.ctypes.data_as(ctypes.c_void_p), t.size, float(rate05),
+                                            float(rate03), int(explicit), int(gauss_width or 0), int(capacity),
+                                            ctypes.byref(h)))
+        self._h, self.n, self.capacity = h, int(n), int(capacity)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _mask_lib().icon_mask_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def filter(self):
+        f = np.zeros((self.n, self.n // 2 + 1), np.float32)
+        _check(_mask_lib().icon_mask_filter(self._h, f.ctypes.data_as(ctypes.c_void_p)))
+        return f
+
+    def apply(self, slices, ystart, thickness):
+        """slices (S, n, n) float32 CUDA tensor -> (S, thickness, n)."""
+        import torch
+        S = slices.shape[0]
+        out = torch.empty((S, thickness, self.n), dtype=torch.float32, device=slices.device)
+        _check(_mask_lib().icon_mask_apply(self._h, ctypes.c_void_p(slices.data_ptr()), S, int(ystart),
+                                           int(thickness), ctypes.c_void_p(out.data_ptr()), _stream()))
+        return out

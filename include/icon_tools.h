@@ -29,6 +29,49 @@ icon_status icon_preprocess(const float *d_in, float *d_out, int nx, int ny, int
 icon_status icon_preprocess_host(const float *h_in, float *h_out, int nx, int ny, int nz, const float *h_tilt_deg,
                                  int thickness);
 
+/* Volume assembly with the cross-validation mask: replaces ICONMask3
+ * (sourceCode/ICONMask3/ICONCrossVMaskIn2D_weightOnlyOnSampled.cu, MK).
+ *
+ * icon_mask_radius: the mask radius as rates of n/2, from the
+ * cross-validation and full-reconstruction FRC curves (frc_len values each,
+ * the second column of crossV.frc / fullRec.frc) when radius < 0 -- the last
+ * frequencies where crossV/fullRec >= 0.5 and >= 0.3 (MK:1033-1100) -- or
+ * from an explicit radius in pixels; invalid curves fall back to the radius
+ * the tilt span fills (MK:996-1005), as the reference does.  *explicit_radius
+ * tells the filter which rule set its Gaussian width (MK:391-411). */
+icon_status icon_mask_radius(int n, const float *tilts, int ntilt, int radius, const float *crossv,
+                             const float *fullrec, int frc_len, float *rate05, float *rate03, int *explicit_radius);
+
+/* Filter for n x n slices (n a power of two, 16..8192): the sampling mask of
+ * the tilts (MK:1107-1139), 1 inside the radius, a Gaussian roll-off of
+ * gauss_width pixels (<= 0: the reference's default) blended with the mask
+ * beyond, times rr / r_full on sampled frequencies (MK:369-468); work space
+ * for `capacity` slices per call on the current device. */
+typedef struct icon_mask icon_mask;
+icon_status icon_mask_create(int n, const float *tilts, int ntilt, float rate05, float rate03, int explicit_radius,
+                             int gauss_width, int capacity, icon_mask **out);
+icon_status icon_mask_destroy(icon_mask *mask);
+
+/* The filter on the half spectrum, [n][n/2+1] floats, into host memory. */
+icon_status icon_mask_filter(const icon_mask *mask, float *h_filter);
+
+/* d_slices [S][n][n] (rows along the thickness) -> d_out [S][thickness][n]:
+ * each slice filtered (R2C, times the filter, C2R, / n^2; MK:479-600) and
+ * rows ystart .. ystart+thickness-1 kept (ystart = n/2 - thickness/2 +
+ * zshift in ICONMask3, MK:1162). */
+icon_status icon_mask_apply(icon_mask *mask, const float *d_slices, int S, int ystart, int thickness, float *d_out,
+                            void *stream);
+
+/* The same on slices in host memory, in batches of the filter's capacity;
+ * allocates and frees device memory and synchronises. */
+icon_status icon_mask_apply_host(icon_mask *mask, const float *h_slices, int S, int ystart, int thickness,
+                                 float *h_out);
+
+/* Assembly without the mask (ICONMask3 -noMask 1, MK:43-368): rows
+ * ystart .. ystart+thickness-1 of every n x n slice. */
+icon_status icon_volume_crop(const float *d_slices, int n, int S, int ystart, int thickness, float *d_out,
+                             void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -113,3 +113,46 @@ def test_preprocess_oracle_matches_reference_tool(name):
     got = pp.preprocess(st, tilts, th)
     ref = z[name + "_normalized"]
     assert np.max(np.abs(got - ref)) <= 2e-6 * np.max(np.abs(ref))
+
+
+MASK_CASES = {
+    # name: (thickness, zshift, radius or None (from the FRC files), gauss width or None, masked)
+    "frc": (64, 0, None, None, True),
+    "radius": (64, 0, 12, 6, True),
+    "crop": (40, 5, 15, None, True),
+    "nomask": (48, 0, None, None, False),
+}
+
+
+@pytest.mark.parametrize("name", list(MASK_CASES))
+def test_mask_oracle_matches_reference_tool(name):
+    # oracle/mask.py against the reference ICONMask3's own output volumes.
+    import oracle.mask as mk
+    z = load_golden("mask")
+    th, zs, radius, gw, masked = MASK_CASES[name]
+    mids, tilts = z["mids"], z["tilts"]
+    n = mids.shape[-1]
+    ystart = n // 2 - th // 2 + zs
+    ref = z["vol_" + name]
+    if not masked:
+        np.testing.assert_array_equal(mk.assemble(mids, ystart, th), ref)
+        return
+    r05, r03, explicit = mk.radius_rates(n, tilts, radius, z["crossV_frc"][:, 1], z["fullRec_frc"][:, 1])
+    filt = mk.half_filter(n, tilts, r05, r03, explicit, gw)
+    got = mk.apply(mids, filt, ystart, th)
+    assert got.shape == ref.shape
+    assert rel_l2(got, ref) < 2e-6
+
+
+@pytest.mark.parametrize("radius", [None, 12, 1000])
+def test_mask_radius_rule_matches_oracle(radius):
+    # The library's host rule (icon_mask_radius, no GPU needed) against the oracle.
+    import oracle.mask as mk
+    from feilab_b200 import tools
+    z = load_golden("mask")
+    cv, fr = z["crossV_frc"][:, 1], z["fullRec_frc"][:, 1]
+    n = z["mids"].shape[-1]
+    got = tools.mask_radius(n, z["tilts"], radius, cv, fr)
+    ref = mk.radius_rates(n, z["tilts"], radius, cv, fr)
+    assert got[2] == ref[2]
+    assert got[0] == pytest.approx(ref[0], rel=1e-7) and got[1] == pytest.approx(ref[1], rel=1e-7)
