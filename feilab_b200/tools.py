@@ -109,3 +109,50 @@ class Mask:
         _check(_mask_lib().icon_mask_apply(self._h, ctypes.c_void_p(slices.data_ptr()), S, int(ystart),
                                            int(thickness), ctypes.c_void_p(out.data_ptr()), _stream()))
         return out
+
+
+def frc(a, b, smooth_overlap=10):
+    """FRC of two (ny, nx) images as the reference's cross validation
+    computes it (calFRC_nonsqure, then frcSmooth); nx/2 values."""
+    L = lib()
+    if not getattr(L, "_frc_ready", False):
+        L.icon_frc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                               ctypes.c_void_p]
+        L.icon_frc.restype = ctypes.c_int
+        L._frc_ready = True
+    a = np.ascontiguousarray(np.asarray(a, np.float32))
+    b = np.ascontiguousarray(np.asarray(b, np.float32))
+    if a.shape != b.shape or a.ndim != 2:
+        raise IconError("frc: two images of the same (ny, nx) shape are needed")
+    ny, nx = a.shape
+    out = np.zeros(nx // 2, np.float32)
+    _check(L.icon_frc(a.ctypes.data_as(ctypes.c_void_p), b.ctypes.data_as(ctypes.c_void_p), nx, ny,
+                      int(smooth_overlap), out.ctypes.data_as(ctypes.c_void_p)))
+    return out
+
+
+def loo_sweep(rows, thickness, tilts, iters=(0, 10, 0), data_type=1, threshold=0.03, capacity=64, tol=0.0,
+              device=0):
+    """Leave-one-out cross validation over every tilt: rows (S, nz, nx)
+    float32 (host).  Returns (frc (nz, nx/2), reprojections (nz, S, nx),
+    iterations per omitted tilt (nz,))."""
+    from .icon import SolveCfg
+    L = lib()
+    if not getattr(L, "_loo_ready", False):
+        V, I = ctypes.c_void_p, ctypes.c_int
+        L.icon_loo_sweep.argtypes = [V, I, I, I, V, ctypes.POINTER(SolveCfg), I, I, ctypes.c_double, I, V, V, V]
+        L.icon_loo_sweep.restype = ctypes.c_int
+        L._loo_ready = True
+    r = np.ascontiguousarray(np.asarray(rows, np.float32))
+    S, nz, nx = r.shape
+    t = np.ascontiguousarray(np.asarray(tilts, np.float32))
+    a, b, c = iters
+    cfg = SolveCfg(int(a), int(b), int(c), int(data_type), float(threshold))
+    f = np.zeros((nz, nx // 2), np.float32)
+    rp = np.zeros((nz, S, nx), np.float32)
+    it = np.zeros(nz, np.int32)
+    _check(L.icon_loo_sweep(r.ctypes.data_as(ctypes.c_void_p), nx, int(thickness), nz, t.ctypes.data_as(ctypes.c_void_p),
+                            ctypes.byref(cfg), S, int(capacity), float(tol), int(device),
+                            f.ctypes.data_as(ctypes.c_void_p), rp.ctypes.data_as(ctypes.c_void_p),
+                            it.ctypes.data_as(ctypes.c_void_p)))
+    return f, rp, it

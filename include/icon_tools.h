@@ -72,6 +72,31 @@ icon_status icon_mask_apply_host(icon_mask *mask, const float *h_slices, int S, 
 icon_status icon_volume_crop(const float *d_slices, int n, int S, int ystart, int thickness, float *d_out,
                              void *stream);
 
+/* Fourier ring correlation of two nx-by-ny images (host memory, nx fastest)
+ * as the reference's cross validation computes it: calFRC_nonsqure
+ * (calFRC.cu:93-174; rings with the y frequency scaled by (nx/ny)^2,
+ * frc[0] = 1) and, with smooth_overlap > 0, frcSmooth (ICONGPU.cu:59-91).
+ * frc_out receives nx/2 values.  Host computation in double. */
+icon_status icon_frc(const float *a, const float *b, int nx, int ny, int smooth_overlap, float *frc_out);
+
+/* Leave-one-out cross validation over every tilt.  The reference validates
+ * one tilt (the smallest |angle|): Lib_2D_crossV2 (MainCode_crossV.cu:3-189)
+ * reconstructs without it, reprojects at its angle and compares with the
+ * omitted projection by FRC.  This call does that for each of the nz tilts
+ * in turn: h_rows [S][nz][nx] (host; rows of every tilt per slice),
+ * thickness, tilt_deg[nz], the solve schedule cfg; plans of `capacity`
+ * slices on `device`.  tol > 0 ends each ICON phase at that relative step
+ * (icon_solve_until); tol = 0 is the reference's solve for every tilt.
+ * Solves start from m = 0: a start holding the omitted projection (the
+ * reconstruction from all tilts, say) would leak it into the validation.
+ * h_frc [nz][nx/2] receives the
+ * smoothed FRC of each omitted tilt; h_reproj [nz][S][nx] (optional) the
+ * reprojections; h_iters[nz] (optional) the iterations of each tilt's
+ * longest batch.  Synchronous. */
+icon_status icon_loo_sweep(const float *h_rows, int nx, int thickness, int nz, const float *tilt_deg,
+                           const icon_solve_cfg *cfg, int S, int capacity, double tol, int device, float *h_frc,
+                           float *h_reproj, int *h_iters);
+
 #ifdef __cplusplus
 }
 #endif

@@ -156,3 +156,19 @@ def test_mask_radius_rule_matches_oracle(radius):
     ref = mk.radius_rates(n, z["tilts"], radius, cv, fr)
     assert got[2] == ref[2]
     assert got[0] == pytest.approx(ref[0], rel=1e-7) and got[1] == pytest.approx(ref[1], rel=1e-7)
+
+
+def test_frc_matches_reference_crossv_file(golden, tmp_path):
+    # icon_frc (host code, no GPU) on the reference ICON-GPU's own
+    # GroundTruth and crossV reprojection reproduces its crossV.frc file.
+    from feilab_b200 import mrc, tools
+    z = golden["cli"]
+    imgs = []
+    for key in ("cli_GroundTruth_mrc", "cli_crossV_reprojection_mrc"):
+        p = tmp_path / (key + ".mrc")
+        p.write_bytes(z[key].tobytes())
+        imgs.append(mrc.read(str(p))[1][0])
+    ref = np.loadtxt(z["cli_crossV_frc"].tobytes().decode().splitlines())
+    got = tools.frc(imgs[0], imgs[1], 10)
+    assert got.shape == (ref.shape[0],)
+    np.testing.assert_allclose(got, ref[:, 1], atol=2e-6)
