@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
@@ -449,12 +450,22 @@ icon_status launch_adjoint(icon_plan *p, const float2 *f_int, int G, int mode, f
     return ICON_OK;
 }
 
-icon_status launch_rows(icon_plan *p, const float *d_rows, int S, int G, float2 *bout, cudaStream_t st)
+// Row transform of S slices; the row of slice sl for tilt i starts at
+// d_rows + sl*sstride + sec*istride, sec = i, or i + 1 from tilt `skip` on.
+icon_status launch_rows_at(icon_plan *p, const float *d_rows, size_t sstride, size_t istride, int skip, int S, int G,
+                           float2 *bout, cudaStream_t st)
 {
     Geo g = p->geo(p->nodes);
-    WITH_B(p->B, LAUNCH(p, K_ROWS, st, L::rows_fwd(p->ex, dim3(p->nz, G), p->thr_x, p->smem_x, st, g, p->geo1(), d_rows, S, p->f, bout)))
+    WITH_B(p->B, LAUNCH(p, K_ROWS, st, L::rows_fwd(p->ex, dim3(p->nz, G), p->thr_x, p->smem_x, st, g, p->geo1(), d_rows,
+                                                   sstride, istride, skip, S, p->f, bout)))
     ICON_CUDA(cudaGetLastError());
     return ICON_OK;
+}
+
+// Rows in the caller layout [S][nz][nx].
+icon_status launch_rows(icon_plan *p, const float *d_rows, int S, int G, float2 *bout, cudaStream_t st)
+{
+    return launch_rows_at(p, d_rows, (size_t)p->nz * p->nx, (size_t)p->nx, INT_MAX, S, G, bout, st);
 }
 
 // One ICON iteration over G groups (Iteration2.cu:53-132 with Alpha2).
@@ -476,6 +487,19 @@ icon_status launch_iteration(icon_plan *p, int G, bool clamp, int data_type, flo
         LAUNCH(p, K_UPD, st, icon::k_step_reduce<<<(slots + 127) / 128, 128, 0, st>>>(p->step_part, (int)gu.x, p->B, slots, p->step));
     }
     ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+// After the row transform of G groups: Ahwb = A^H W b, m = 0, the schedule's
+// iterations (MainCode.cu:115-140 with Iteration3).
+icon_status solve_from_rows(icon_plan *p, const icon_solve_cfg *cfg, int G, cudaStream_t st)
+{
+    const int a = cfg->infr_before, b = cfg->icon, c = cfg->infr_after, iters = a + b + c;
+    ICON_TRY(launch_adjoint(p, p->f, G, 0, p->Ahwb, st));
+    size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
+    ICON_CUDA(cudaMemsetAsync(p->m, 0, tot * sizeof(float), st));
+    for (int it = 0; it < iters; ++it)
+        ICON_TRY(launch_iteration(p, G, a <= it && it < iters - c, cfg->data_type, cfg->threshold, nullptr, nullptr, st));
     return ICON_OK;
 }
 
@@ -772,6 +796,170 @@ icon_status icon_prepare_rhs(icon_plan *p, const float *d_rows, void *d_Ahwb, in
     return ICON_OK;
 }
 
+// Stack arguments shared by the two stack entry points: the plan's tilts
+// read sections 0..nz-1 of the stack, or nz+1 sections with skip_section
+// left out.
+static icon_status check_stack(const icon_plan *p, const float *d_stack, int ny, int y0, int skip_section, int S)
+{
+    if (!d_stack) return fail(ICON_ERR_INVALID, "null stack");
+    if (ny < 1 || y0 < 0 || S < 1 || (long long)y0 + S > ny)
+        return fail(ICON_ERR_INVALID, "slices " + std::to_string(y0) + "..+" + std::to_string(S) + " outside 0.." +
+                                          std::to_string(ny - 1));
+    if (skip_section > p->nz) return fail(ICON_ERR_INVALID, "skip_section beyond the stack");
+    return ICON_OK;
+}
+
+icon_status icon_prepare_rhs_stack(icon_plan *p, const float *d_stack, int ny, int y0, int skip_section,
+                                   void *d_Ahwb, int S, void *stream)
+{
+    ICON_TRY(check_plan(p, S));
+    ICON_TRY(check_stack(p, d_stack, ny, y0, skip_section, S));
+    if (!d_Ahwb) return fail(ICON_ERR_INVALID, "null buffer");
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    int G = groups(p, S);
+    const size_t nx = p->nx;
+    ICON_TRY(launch_rows_at(p, d_stack + (size_t)y0 * nx, nx, (size_t)ny * nx, skip_section < 0 ? INT_MAX : skip_section,
+                            S, G, nullptr, st));
+    ICON_TRY(launch_adjoint(p, p->f, G, 0, p->imgc, st));
+    LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float2><<<grid1d((size_t)S * p->N0 * p->N1), 256, 0, st>>>(p->imgc, (float2 *)d_Ahwb, S, p->N0, p->N1, p->B));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+icon_status icon_reconstruct_stack(icon_plan *p, const icon_solve_cfg *cfg, const float *d_stack, int ny, int y0,
+                                   int skip_section, float *d_slices, float *d_reproj, int S, void *stream)
+{
+    if (!p || !cfg) return fail(ICON_ERR_INVALID, "null argument");
+    if (!d_slices && !d_reproj) return fail(ICON_ERR_INVALID, "no output buffer");
+    ICON_TRY(check_stack(p, d_stack, ny, y0, skip_section, S));
+    if (cfg->infr_before < 0 || cfg->icon < 0 || cfg->infr_after < 0) return fail(ICON_ERR_INVALID, "negative iteration count");
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t nx = p->nx, NN = (size_t)p->N0 * p->N1;
+    const int skip = skip_section < 0 ? INT_MAX : skip_section;
+    for (int s0 = 0; s0 < S; s0 += p->cap) {
+        const int Sc = std::min(p->cap, S - s0), G = groups(p, Sc);
+        ICON_TRY(launch_rows_at(p, d_stack + (size_t)(y0 + s0) * nx, nx, (size_t)ny * nx, skip, Sc, G, nullptr, st));
+        ICON_TRY(solve_from_rows(p, cfg, G, st));
+        if (d_slices) {
+            dim3 gl((unsigned)std::min<size_t>(((size_t)G * NN + 255) / 256, 4096));
+            WITH_B(p->B, LAUNCH(p, K_LAYOUT, st, L::img_out_file(gl, st, p->m, d_slices + (size_t)s0 * NN, Sc, p->N0, p->N1)))
+            ICON_CUDA(cudaGetLastError());
+        }
+        if (d_reproj) ICON_TRY(reproject_internal(p, p->m, p->reproj_deg, d_reproj + (size_t)s0 * nx, Sc, st));
+    }
+    return ICON_OK;
+}
+
+icon_status icon_reconstruct_stack_host(icon_plan *p, const icon_solve_cfg *cfg, const float *d_stack, int ny, int y0,
+                                        int skip_section, int S, int outputs, icon_batch_sink sink, void *ctx,
+                                        void *stream)
+{
+    if (!p || !cfg || !sink) return fail(ICON_ERR_INVALID, "null argument");
+    if ((outputs & 3) == 0 || (outputs & ~3)) return fail(ICON_ERR_INVALID, "outputs must be a nonempty set of ICON_OUT_* bits");
+    ICON_TRY(check_stack(p, d_stack, ny, y0, skip_section, S));
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    bool own = (st == nullptr);
+    if (own) ICON_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    const size_t NN = (size_t)p->N0 * p->N1, nx = p->nx;
+    const bool want_m = outputs & ICON_OUT_SLICES, want_rp = outputs & ICON_OUT_REPROJECTION;
+    // Two pinned host buffers (slices, then reprojections) and two events:
+    // batch k copies into buffer k % 2 while the sink consumes batch k - 1.
+    float *h[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    const size_t per = (want_m ? (size_t)p->cap * NN : 0) + (want_rp ? (size_t)p->cap * nx : 0);
+    icon_status rc = ICON_OK;
+    for (int k = 0; k < 2 && rc == ICON_OK; ++k) {
+        cudaError_t e = cudaHostAlloc((void **)&h[k], per * sizeof(float), cudaHostAllocDefault);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
+        if (e != cudaSuccess) rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+    }
+    auto hm = [&](int k) { return h[k]; };
+    auto hr = [&](int k) { return h[k] + (want_m ? (size_t)p->cap * NN : 0); };
+    int pend_s0 = -1, pend_n = 0, pend_k = 0;
+    auto drain = [&]() -> icon_status {      // waits for the pending batch and hands it to the sink
+        if (pend_s0 < 0) return ICON_OK;
+        ICON_CUDA(cudaEventSynchronize(ev[pend_k]));
+        int r = sink(ctx, pend_s0, pend_n, want_m ? hm(pend_k) : nullptr, want_rp ? hr(pend_k) : nullptr);
+        pend_s0 = -1;
+        if (r != 0) return fail(ICON_ERR_INVALID, "the batch sink returned " + std::to_string(r));
+        return ICON_OK;
+    };
+    for (int s0 = 0, k = 0; s0 < S && rc == ICON_OK; s0 += p->cap, k ^= 1) {
+        const int Sc = std::min(p->cap, S - s0);
+        rc = icon_reconstruct_stack(p, cfg, d_stack, ny, y0 + s0, skip_section, want_m ? p->mout : nullptr,
+                                    want_rp ? p->outrp : nullptr, Sc, st);
+        cudaError_t e = cudaSuccess;
+        if (rc == ICON_OK && want_m) e = cudaMemcpyAsync(hm(k), p->mout, sizeof(float) * NN * Sc, cudaMemcpyDeviceToHost, st);
+        if (rc == ICON_OK && e == cudaSuccess && want_rp)
+            e = cudaMemcpyAsync(hr(k), p->outrp, sizeof(float) * nx * Sc, cudaMemcpyDeviceToHost, st);
+        if (rc == ICON_OK && e == cudaSuccess) e = cudaEventRecord(ev[k], st);
+        if (rc == ICON_OK && e != cudaSuccess) rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+        if (rc == ICON_OK) rc = drain();     // batch k - 1, while batch k runs
+        pend_s0 = s0;
+        pend_n = Sc;
+        pend_k = k;
+    }
+    if (rc == ICON_OK) rc = drain();
+    cudaStreamSynchronize(st);
+    for (int k = 0; k < 2; ++k) {
+        if (h[k]) cudaFreeHost(h[k]);
+        if (ev[k]) cudaEventDestroy(ev[k]);
+    }
+    if (own) cudaStreamDestroy(st);
+    return rc;
+}
+
+icon_status icon_host_alloc(size_t bytes, void **out)
+{
+    if (!out) return fail(ICON_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (bytes == 0) return fail(ICON_ERR_INVALID, "zero bytes");
+    ICON_CUDA(cudaHostAlloc(out, bytes, cudaHostAllocPortable));
+    return ICON_OK;
+}
+
+icon_status icon_host_free(void *h)
+{
+    if (h) ICON_CUDA(cudaFreeHost(h));
+    return ICON_OK;
+}
+
+icon_status icon_stack_upload(int device, const float *h_stack, int sections, int ny, int nx, int y0, int S,
+                              float **d_stack, void *stream)
+{
+    if (!h_stack || !d_stack) return fail(ICON_ERR_INVALID, "null argument");
+    *d_stack = nullptr;
+    if (sections < 1 || ny < 1 || nx < 1 || y0 < 0 || S < 1 || (long long)y0 + S > ny)
+        return fail(ICON_ERR_INVALID, "stack rows outside the stack");
+    DeviceGuard guard(device);
+    if (!guard.ok) return fail(ICON_ERR_CUDA, "cannot select device " + std::to_string(device));
+    float *d = nullptr;
+    ICON_CUDA(cudaMalloc(&d, sizeof(float) * (size_t)sections * S * nx));
+    // One 2-D copy: per section, the S rows y0 .. y0+S-1 (contiguous in the
+    // file), to a packed [sections][S][nx].
+    cudaError_t e = cudaMemcpy2DAsync(d, sizeof(float) * (size_t)S * nx, h_stack + (size_t)y0 * nx,
+                                      sizeof(float) * (size_t)ny * nx, sizeof(float) * (size_t)S * nx, sections,
+                                      cudaMemcpyHostToDevice, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+    }
+    *d_stack = d;
+    return ICON_OK;
+}
+
+icon_status icon_device_free(int device, void *d)
+{
+    if (!d) return ICON_OK;
+    DeviceGuard guard(device);
+    ICON_CUDA(cudaFree(d));
+    return ICON_OK;
+}
+
 icon_status icon_solve(icon_plan *p, const icon_solve_cfg *cfg, const void *d_Ahwb, float *d_m, int S, int warm_start,
                        double *h_alpha, double *h_rtr, void *stream)
 {
@@ -894,19 +1082,14 @@ icon_status icon_reconstruct_host(icon_plan *p, const icon_solve_cfg *cfg, const
     icon_status rc = ICON_OK;
     size_t R = (size_t)p->nz * p->nx, NN = (size_t)p->N0 * p->N1;
     float *d_mo = p->mout;
-    int a = cfg->infr_before, b = cfg->icon, c = cfg->infr_after, iters = a + b + c;
+    if (cfg->infr_before < 0 || cfg->icon < 0 || cfg->infr_after < 0) return fail(ICON_ERR_INVALID, "negative iteration count");
     for (int s0 = 0; s0 < S && rc == ICON_OK; s0 += p->cap) {
         int Sc = std::min(p->cap, S - s0);
         int G = groups(p, Sc);
         cudaError_t e = cudaMemcpyAsync(p->rows, h_rows + (size_t)s0 * R, sizeof(float) * R * Sc, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) { rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e)); break; }
         if ((rc = launch_rows(p, p->rows, Sc, G, nullptr, st)) != ICON_OK) break;
-        if ((rc = launch_adjoint(p, p->f, G, 0, p->Ahwb, st)) != ICON_OK) break;
-        size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
-        if ((e = cudaMemsetAsync(p->m, 0, tot * sizeof(float), st)) != cudaSuccess) { rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e)); break; }
-        for (int it = 0; it < iters && rc == ICON_OK; ++it)
-            rc = launch_iteration(p, G, a <= it && it < iters - c, cfg->data_type, cfg->threshold, nullptr, nullptr, st);
-        if (rc != ICON_OK) break;
+        if ((rc = solve_from_rows(p, cfg, G, st)) != ICON_OK) break;
         LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float><<<grid1d((size_t)Sc * NN), 256, 0, st>>>(p->m, d_mo, Sc, p->N0, p->N1, p->B));
         if (h_reproj && (rc = reproject_internal(p, p->m, p->reproj_deg, p->outrp, Sc, st)) != ICON_OK) break;
         if ((e = cudaMemcpyAsync(h_m + (size_t)s0 * NN, d_mo, sizeof(float) * NN * Sc, cudaMemcpyDeviceToHost, st)) != cudaSuccess) {

@@ -67,10 +67,68 @@ struct Job {
 
 std::string join(const std::string &a, const std::string &b) { return a + "/" + b; }
 
+// Output side of one GPU's full reconstruction: the batch sink of
+// icon_reconstruct_stack_host.  Slices arrive X fastest, so each file is
+// written straight from the pinned buffer while the GPU solves the next batch.
+struct FullSink {
+    const Job *job;
+    const Args *A;
+    const MrcHeader *inh;
+    int thickness;
+    const std::string *recdir;
+    std::vector<float> *volume, *rp_full;
+    std::chrono::steady_clock::time_point last;
+    std::string err;
+};
+
+int full_sink(void *ctx, int s0, int count, const float *h_slices, const float *h_reproj)
+{
+    FullSink &c = *static_cast<FullSink *>(ctx);
+    const int nx = c.inh->nx;
+    const size_t NN = (size_t)nx * c.thickness;
+    auto now = std::chrono::steady_clock::now();
+    double dt = std::chrono::duration<double>(now - c.last).count() / count;
+    c.last = now;
+    for (int s = 0; s < count; ++s) {
+        const int y = c.job->y0 + s0 + s;
+        const float *slice = h_slices + (size_t)s * NN;
+        MrcHeader oh = *c.inh;                           // saveMRC_real.cu:37-46
+        oh.mz = c.inh->mx;
+        oh.zlen = c.inh->xlen;
+        oh.nx = nx;
+        oh.ny = c.thickness;
+        oh.nz = 1;
+        char name[64];
+        snprintf(name, sizeof name, "mid%05d.mrc", y);
+        if (!mrc_write_float(join(*c.recdir, name), oh, slice, c.err)) return 1;
+        if (c.volume) std::memcpy(&(*c.volume)[(size_t)(y - c.A->ystart) * NN], slice, sizeof(float) * NN);
+        std::memcpy(&(*c.rp_full)[(size_t)(y - c.A->ystart) * nx], h_reproj + (size_t)s * nx, sizeof(float) * nx);
+        printf("slice %d finished, time %lf\n", y, dt);
+    }
+    return 0;
+}
+
+struct CvSink {
+    const Job *job;
+    const Args *A;
+    int nx;
+    std::vector<float> *rp_cv;
+};
+
+int cv_sink(void *ctx, int s0, int count, const float *, const float *h_reproj)
+{
+    CvSink &c = *static_cast<CvSink *>(ctx);
+    std::memcpy(&(*c.rp_cv)[(size_t)(c.job->y0 + s0 - c.A->ystart) * c.nx], h_reproj, sizeof(float) * c.nx * count);
+    return 0;
+}
+
 // One GPU's share: reconstruct slices [y0, y1) (and, unless skipped, the
 // cross-validation solve), write the slice files, fill the reprojections.
+// The GPU gets the share's rows of every section in one copy (the reference
+// reads each slice's rows from the file pixel by pixel, readSlicePart.cu:3-31
+// over mrcfile3.c:902-951) and both solves read them from there.
 void run_job(Job &job, const Args &A, const MrcHeader &inh, const std::vector<float> &tilts, int thickness,
-             const std::vector<float> &stack, int omit, std::vector<float> &rp_full, std::vector<float> &rp_cv,
+             const float *stack, int omit, std::vector<float> &rp_full, std::vector<float> &rp_cv,
              std::vector<float> *volume, const std::string &recdir)
 {
     const int nx = inh.nx, ny = inh.ny, nz = inh.nz;
@@ -78,60 +136,37 @@ void run_job(Job &job, const Args &A, const MrcHeader &inh, const std::vector<fl
     if (S <= 0) return;
     icon_solve_cfg cfg{A.iters[0], A.iters[1], A.iters[2], A.data_type, A.threshold};
     const int cap = std::min(A.batch, S);
-    const size_t NN = (size_t)nx * thickness;
     auto fail = [&](const std::string &m) {
         job.rc = 1;
         job.err = m + ": " + icon_last_error();
     };
+    float *d_stack = nullptr;
+    if (icon_stack_upload(job.device, stack, nz, ny, nx, job.y0, S, &d_stack, nullptr) != ICON_OK)
+        return fail("stack upload");
+    struct Free {
+        int dev;
+        float *p;
+        ~Free() { icon_device_free(dev, p); }
+    } free_stack{job.device, d_stack};
     // Full reconstruction (Lib_2D2, MainCode.cu:3-177).
     {
         icon_geometry g{nx, thickness, nz, tilts.data(), cap, job.device};
         icon_plan *plan = nullptr;
         if (icon_plan_create(&g, &plan) != ICON_OK) return fail("plan");
-        std::vector<float> rows((size_t)cap * nz * nx), m((size_t)cap * NN), rp((size_t)cap * nx);
-        for (int s0 = 0; s0 < S; s0 += cap) {
-            int sc = std::min(cap, S - s0);
-            for (int s = 0; s < sc; ++s)
-                for (int i = 0; i < nz; ++i)
-                    std::memcpy(&rows[((size_t)s * nz + i) * nx], &stack[((size_t)i * ny + job.y0 + s0 + s) * nx],
-                                sizeof(float) * nx);
-            auto t0 = std::chrono::steady_clock::now();
-            if (icon_reconstruct_host(plan, &cfg, rows.data(), m.data(), rp.data(), sc, nullptr) != ICON_OK) {
-                icon_plan_destroy(plan);
-                return fail("reconstruction");
-            }
-            double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-            std::vector<float> slice(NN);
-            for (int s = 0; s < sc; ++s) {
-                int y = job.y0 + s0 + s;
-                const float *ms = &m[(size_t)s * NN];
-                for (int j = 0; j < thickness; ++j)          // saveMRC_real_inv: X fastest
-                    for (int i = 0; i < nx; ++i) slice[(size_t)j * nx + i] = ms[(size_t)i * thickness + j];
-                MrcHeader oh = inh;                           // saveMRC_real.cu:37-46
-                oh.mz = inh.mx;
-                oh.zlen = inh.xlen;
-                oh.nx = nx;
-                oh.ny = thickness;
-                oh.nz = 1;
-                char name[64];
-                snprintf(name, sizeof name, "mid%05d.mrc", y);
-                std::string e;
-                if (!mrc_write_float(join(recdir, name), oh, slice.data(), e)) {
-                    icon_plan_destroy(plan);
-                    job.rc = 1;
-                    job.err = e;
-                    return;
-                }
-                if (volume) std::memcpy(&(*volume)[(size_t)(y - A.ystart) * NN], slice.data(), sizeof(float) * NN);
-                std::memcpy(&rp_full[(size_t)(y - A.ystart) * nx], &rp[(size_t)s * nx], sizeof(float) * nx);
-                printf("slice %d finished, time %lf\n", y, dt / sc);
-            }
-        }
+        FullSink sink{&job, &A, &inh, thickness, &recdir, volume, &rp_full, std::chrono::steady_clock::now(), {}};
+        icon_status rc = icon_reconstruct_stack_host(plan, &cfg, d_stack, S, 0, -1, S,
+                                                     ICON_OUT_SLICES | ICON_OUT_REPROJECTION, full_sink, &sink, nullptr);
         icon_plan_destroy(plan);
+        if (rc != ICON_OK) {
+            job.rc = 1;
+            job.err = sink.err.empty() ? std::string("reconstruction: ") + icon_last_error() : sink.err;
+            return;
+        }
     }
     if (A.skip_cv) return;
     // Cross-validation solve without the smallest-|angle| tilt, reprojected
-    // at that tilt (Lib_2D_crossV2, MainCode_crossV.cu:3-189).
+    // at that tilt (Lib_2D_crossV2, MainCode_crossV.cu:3-189); the stack's
+    // section `omit` is skipped on the device.
     std::vector<float> t2;
     for (int i = 0; i < nz; ++i)
         if (i != omit) t2.push_back(tilts[i]);
@@ -142,24 +177,11 @@ void run_job(Job &job, const Args &A, const MrcHeader &inh, const std::vector<fl
         icon_plan_destroy(plan);
         return fail("cross-validation reprojection angle");
     }
-    std::vector<float> rows((size_t)cap * (nz - 1) * nx), m((size_t)cap * NN), rp((size_t)cap * nx);
-    for (int s0 = 0; s0 < S; s0 += cap) {
-        int sc = std::min(cap, S - s0);
-        for (int s = 0; s < sc; ++s)
-            for (int i = 0, k = 0; i < nz; ++i) {
-                if (i == omit) continue;
-                std::memcpy(&rows[((size_t)s * (nz - 1) + k) * nx], &stack[((size_t)i * ny + job.y0 + s0 + s) * nx],
-                            sizeof(float) * nx);
-                ++k;
-            }
-        if (icon_reconstruct_host(plan, &cfg, rows.data(), m.data(), rp.data(), sc, nullptr) != ICON_OK) {
-            icon_plan_destroy(plan);
-            return fail("cross-validation reconstruction");
-        }
-        for (int s = 0; s < sc; ++s)
-            std::memcpy(&rp_cv[(size_t)(job.y0 + s0 + s - A.ystart) * nx], &rp[(size_t)s * nx], sizeof(float) * nx);
-    }
+    CvSink sink{&job, &A, nx, &rp_cv};
+    icon_status rc = icon_reconstruct_stack_host(plan, &cfg, d_stack, S, 0, omit, S, ICON_OUT_REPROJECTION, cv_sink,
+                                                 &sink, nullptr);
     icon_plan_destroy(plan);
+    if (rc != ICON_OK) fail("cross-validation reconstruction");
 }
 
 bool next_arg(int argc, char **argv, int &i, std::string &v)
@@ -283,8 +305,23 @@ int main(int argc, char **argv)
         return 1;
     }
     const int thickness = A.thickness == 0 ? inh.nx : A.thickness;   // MainCode.cu:14-16
-    std::vector<float> stack;
-    if (!mrc_read_sections(A.input, inh, 0, inh.nz, stack, err)) {
+    // The whole stack in one read, into pinned memory when it can be had.
+    const size_t stack_n = (size_t)inh.nx * inh.ny * inh.nz;
+    std::vector<float> stack_pageable;
+    float *stack = nullptr;
+    if (icon_host_alloc(sizeof(float) * stack_n, (void **)&stack) != ICON_OK) {
+        stack_pageable.resize(stack_n);
+        stack = stack_pageable.data();
+    }
+    struct FreeHost {
+        float *p;
+        bool pinned;
+        ~FreeHost()
+        {
+            if (pinned) icon_host_free(p);
+        }
+    } free_host{stack, stack_pageable.empty()};
+    if (!mrc_read_sections_into(A.input, inh, 0, inh.nz, stack, err)) {
         printf("%s\n", err.c_str());
         return 1;
     }

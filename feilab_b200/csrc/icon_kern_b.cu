@@ -66,10 +66,17 @@ void Launch<B>::xpass_adj(int mode, int E, dim3 grid, int threads, size_t smem, 
 
 template <int B>
 void Launch<B>::rows_fwd(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const Geo1 &g1,
-                         const float *rows, int S, float2 *f, float2 *bout)
+                         const float *rows, size_t sstride, size_t istride, int skip, int S, float2 *f,
+                         float2 *bout)
 {
-    if (E == 32) k_rows_fwd<B, 32><<<grid, threads, smem, st>>>(g, g1, rows, S, f, bout);
-    else k_rows_fwd<B, 16><<<grid, threads, smem, st>>>(g, g1, rows, S, f, bout);
+    if (E == 32) k_rows_fwd<B, 32><<<grid, threads, smem, st>>>(g, g1, rows, sstride, istride, skip, S, f, bout);
+    else k_rows_fwd<B, 16><<<grid, threads, smem, st>>>(g, g1, rows, sstride, istride, skip, S, f, bout);
+}
+
+template <int B>
+void Launch<B>::img_out_file(dim3 grid, cudaStream_t st, const float *m, float *out, int S, int N0, int N1)
+{
+    k_img_out_file<B><<<grid, 256, 0, st>>>(m, out, S, N0, N1);
 }
 
 template <int B>

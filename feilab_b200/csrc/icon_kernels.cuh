@@ -603,19 +603,25 @@ __global__ void FFT_BOUNDS(E) k_xpass_adj(Geo g, const float2 *__restrict__ G1, 
 // Input stage: per (tilt i, group) the 1-D NUFFT of the projection rows
 // (cunfft_trafo_1d NU:1479-1516: pre-pass NU:1432-1452, FFT, interpolation
 // NU:1454-1477 with taps summed in order), then f = b*w (NU:1539-1549).
-// rows: [S][nz][nx] (caller layout).  f, bout: [G][M][B]; bout may be null.
+// Row of slice sl for tilt i: rows[sl*sstride + sec*istride .. + nx), with
+// sec = i, or i + 1 from tilt `skip` on (a stack section left out).  The
+// caller layout [S][nz][nx] is sstride = nz*nx, istride = nx; a tilt stack
+// in file order [sections][ny][nx] is sstride = nx, istride = ny*nx.
+// f, bout: [G][M][B]; bout may be null.
 template <int B, int E>
-__global__ void FFT_BOUNDS(E) k_rows_fwd(Geo g, Geo1 g1, const float *__restrict__ rows, int S,
-                                         float2 *__restrict__ f, float2 *__restrict__ bout)
+__global__ void FFT_BOUNDS(E) k_rows_fwd(Geo g, Geo1 g1, const float *__restrict__ rows, size_t sstride,
+                                         size_t istride, int skip, int S, float2 *__restrict__ f,
+                                         float2 *__restrict__ bout)
 {
     extern __shared__ float2 s[];
     constexpr int LB = Log2B<B>::v;
-    const int i = blockIdx.x, grp = blockIdx.y, n = g.n0, N = g.nx, nz = g.nz;
+    const int i = blockIdx.x, grp = blockIdx.y, n = g.n0, N = g.nx;
     const float *rcx = g.rcx;
+    const float *rowi = rows + (size_t)(i < skip ? i : i + 1) * istride;
     for (int idx = threadIdx.x; idx < N * B; idx += blockDim.x) {
         int b = idx / N, X = idx % N;                      // coalesced along X
         int sl = grp * B + b;
-        s[X * B + b] = make_float2(sl < S ? rows[((size_t)sl * nz + i) * N + X] * rcx[X] : 0.f, 0.f);
+        s[X * B + b] = make_float2(sl < S ? rowi[(size_t)sl * sstride + X] * rcx[X] : 0.f, 0.f);
     }
     __syncthreads();
     auto ld = [=](int x, int b) -> float2 {
@@ -705,6 +711,41 @@ __global__ void k_img_in(const T *__restrict__ src, T *__restrict__ dst, int S, 
         T v{};
         if (sl < S) v = src[((size_t)sl * N0 + X) * N1 + Y];
         dst[o] = v;
+    }
+}
+
+// Batched image [G][N1][N0][B] -> file layout [S][N1][N0] (X fastest, the
+// order saveMRC_real_inv writes a slice in, saveMRC_real.cu:49-53).  One
+// thread per (Y, X) reads the B values of the point (one 32-byte run for
+// B = 8) and writes them to the B slices, each store coalesced along X.
+template <int B>
+__global__ void k_img_out_file(const float *__restrict__ src, float *__restrict__ dst, int S, int N0, int N1)
+{
+    const size_t plane = (size_t)N0 * N1;
+    const int G = (S + B - 1) / B;
+    const size_t total = (size_t)G * plane;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int grp = (int)(i / plane);
+        const size_t yx = i - (size_t)grp * plane;
+        float v[B];
+        if constexpr (B % 4 == 0) {
+#pragma unroll
+            for (int q = 0; q < B / 4; ++q) {
+                float4 t = reinterpret_cast<const float4 *>(src + i * B)[q];
+                v[4 * q] = t.x;
+                v[4 * q + 1] = t.y;
+                v[4 * q + 2] = t.z;
+                v[4 * q + 3] = t.w;
+            }
+        } else {
+#pragma unroll
+            for (int b = 0; b < B; ++b) v[b] = src[i * B + b];
+        }
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const int sl = grp * B + b;
+            if (sl < S) dst[(size_t)sl * plane + yx] = v[b];
+        }
     }
 }
 

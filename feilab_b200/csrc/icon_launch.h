@@ -21,7 +21,9 @@ struct Launch {
     static void xpass_adj(int mode, int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
                           const float2 *G1, float2 *out, const float2 *Ahwb, double *part);
     static void rows_fwd(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const Geo1 &g1,
-                         const float *rows, int S, float2 *f, float2 *bout);
+                         const float *rows, size_t sstride, size_t istride, int skip, int S, float2 *f,
+                         float2 *bout);
+    static void img_out_file(dim3 grid, cudaStream_t st, const float *m, float *out, int S, int N0, int N1);
     static void row_adj(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const Geo1 &g1,
                         const float2 *f, float *out, int S);
     static void update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat, const double *alpha, int per_group,

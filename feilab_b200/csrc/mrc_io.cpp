@@ -47,8 +47,8 @@ bool mrc_read_header(const std::string &path, MrcHeader &h, std::string &err)
     return true;
 }
 
-bool mrc_read_sections(const std::string &path, const MrcHeader &h, int z0, int z1, std::vector<float> &out,
-                       std::string &err)
+bool mrc_read_sections_into(const std::string &path, const MrcHeader &h, int z0, int z1, float *out,
+                            std::string &err)
 {
     File fl;
     fl.f = fopen(path.c_str(), "rb");
@@ -70,36 +70,54 @@ bool mrc_read_sections(const std::string &path, const MrcHeader &h, int z0, int 
         return false;
     }
     size_t n = sec * (size_t)(z1 - z0);
-    std::vector<unsigned char> raw(n * ps);
     fseeko(fl.f, start + (long long)z0 * sec * ps, SEEK_SET);
-    if (n && fread(raw.data(), ps, n, fl.f) != n) {
-        err = "short read of " + path;
-        return false;
+    if (h.mode == MRC_FLOAT) {                // straight into the caller's buffer
+        if (n && fread(out, 4, n, fl.f) != n) {
+            err = "short read of " + path;
+            return false;
+        }
+        return true;
     }
-    out.resize(n);
-    switch (h.mode) {
-    case MRC_BYTE:
-        for (size_t i = 0; i < n; ++i) out[i] = (float)raw[i];
-        break;
-    case MRC_SHORT:
-        for (size_t i = 0; i < n; ++i) {
-            int16_t v;
-            std::memcpy(&v, &raw[2 * i], 2);
-            out[i] = (float)v;
+    // Integer modes: read in blocks of one section and convert.
+    std::vector<unsigned char> raw(sec * ps);
+    for (size_t done = 0; done < n; done += sec) {
+        if (fread(raw.data(), ps, sec, fl.f) != sec) {
+            err = "short read of " + path;
+            return false;
         }
-        break;
-    case MRC_USHORT:
-        for (size_t i = 0; i < n; ++i) {
-            uint16_t v;
-            std::memcpy(&v, &raw[2 * i], 2);
-            out[i] = (float)v;
+        float *o = out + done;
+        switch (h.mode) {
+        case MRC_BYTE:
+            for (size_t i = 0; i < sec; ++i) o[i] = (float)raw[i];
+            break;
+        case MRC_SHORT:
+            for (size_t i = 0; i < sec; ++i) {
+                int16_t v;
+                std::memcpy(&v, &raw[2 * i], 2);
+                o[i] = (float)v;
+            }
+            break;
+        default:   // MRC_USHORT
+            for (size_t i = 0; i < sec; ++i) {
+                uint16_t v;
+                std::memcpy(&v, &raw[2 * i], 2);
+                o[i] = (float)v;
+            }
+            break;
         }
-        break;
-    default:
-        std::memcpy(out.data(), raw.data(), n * 4);
-        break;
     }
     return true;
+}
+
+bool mrc_read_sections(const std::string &path, const MrcHeader &h, int z0, int z1, std::vector<float> &out,
+                       std::string &err)
+{
+    if (z0 < 0 || z1 > h.nz || z0 > z1) {
+        err = "section range out of bounds";
+        return false;
+    }
+    out.resize((size_t)h.nx * h.ny * (z1 - z0));
+    return mrc_read_sections_into(path, h, z0, z1, out.data(), err);
 }
 
 bool mrc_write_float(const std::string &path, MrcHeader h, const float *data, std::string &err)

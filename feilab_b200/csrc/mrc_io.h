@@ -47,6 +47,11 @@ bool mrc_read_header(const std::string &path, MrcHeader &h, std::string &err);
 bool mrc_read_sections(const std::string &path, const MrcHeader &h, int z0, int z1, std::vector<float> &out,
                        std::string &err);
 
+// The same into out[(z1 - z0) * ny * nx] (e.g. pinned memory): one read for
+// float files, one section at a time for the integer modes.
+bool mrc_read_sections_into(const std::string &path, const MrcHeader &h, int z0, int z1, float *out,
+                            std::string &err);
+
 // Writes a float file with header `h` (nx, ny, nz, mode set by the caller;
 // `next` bytes of zeros follow the header) and the statistics amin, amax,
 // amean and rms recomputed from the data as mrc_update_head does

@@ -47,6 +47,13 @@ def lib():
                                        ctypes.POINTER(I), V, V]
         L.icon_reproject.argtypes = [P, V, F, V, I, V]
         L.icon_reconstruct_host.argtypes = [P, ctypes.POINTER(SolveCfg), V, V, V, I, V]
+        L.icon_prepare_rhs_stack.argtypes = [P, V, I, I, I, V, I, V]
+        L.icon_reconstruct_stack.argtypes = [P, ctypes.POINTER(SolveCfg), V, I, I, I, V, V, I, V]
+        L.icon_reconstruct_stack_host.argtypes = [P, ctypes.POINTER(SolveCfg), V, I, I, I, I, I, BATCH_SINK, V, V]
+        L.icon_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(V)]
+        L.icon_host_free.argtypes = [V]
+        L.icon_stack_upload.argtypes = [I, V, I, I, I, I, I, ctypes.POINTER(V), V]
+        L.icon_device_free.argtypes = [I, V]
         L.icon_trace_enable.argtypes = [P, I]
         L.icon_trace_read.argtypes = [P, V, V, V]
         L.icon_launch_count.argtypes = [P]
@@ -55,10 +62,18 @@ def lib():
         for name in ("icon_plan_create", "icon_plan_destroy", "icon_plan_query", "icon_plan_geometry",
                      "icon_nufft_forward", "icon_nufft_forward_complex", "icon_nufft_adjoint",
                      "icon_rows_forward", "icon_prepare_rhs", "icon_solve", "icon_solve_until", "icon_reproject",
-                     "icon_reconstruct_host", "icon_trace_enable", "icon_trace_read"):
+                     "icon_reconstruct_host", "icon_trace_enable", "icon_trace_read", "icon_prepare_rhs_stack",
+                     "icon_reconstruct_stack", "icon_reconstruct_stack_host", "icon_host_alloc", "icon_host_free",
+                     "icon_stack_upload", "icon_device_free"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
+
+
+# icon_batch_sink: int (*)(void *ctx, int s0, int count, const float *h_slices, const float *h_reproj)
+BATCH_SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                              ctypes.c_void_p)
+OUT_SLICES, OUT_REPROJECTION = 1, 2
 
 
 class Geometry(ctypes.Structure):
@@ -241,6 +256,66 @@ class IconPlan:
                                            rp.ctypes.data_as(ctypes.c_void_p) if reproject else None, S, st))
         return (out, rp) if reproject else out
 
+    def prepare_rhs_stack(self, stack, y0, S, skip_section=-1):
+        """A^H W b of slices y0 .. y0+S-1 read from a device tilt stack
+        (sections, ny, nx) float32 in file order; skip_section >= 0 leaves
+        that section out (the stack then has one section more than the plan
+        has tilts).  -> (S, N0, N1) complex64."""
+        import torch
+        stack = self._dev(stack, torch.float32)
+        out = torch.empty((S, self.N0, self.N1), dtype=torch.complex64, device=self.device)
+        _check(lib().icon_prepare_rhs_stack(self._h, _ptr(stack), stack.shape[1], int(y0), int(skip_section), _ptr(out),
+                                            int(S), _stream()))
+        return out
+
+    def reconstruct_stack(self, stack, y0, S, iters=(0, 10, 0), data_type=1, threshold=0.03, skip_section=-1,
+                          slices=True, reproject=False):
+        """The solve of slices y0 .. y0+S-1 of a device tilt stack, on the
+        device: slices (S, N1, N0) float32 in file layout (X fastest) and/or
+        the reprojection (S, nx) at the plan's reprojection angle."""
+        import torch
+        stack = self._dev(stack, torch.float32)
+        a, b, c = iters
+        cfg = SolveCfg(int(a), int(b), int(c), int(data_type), float(threshold))
+        m = torch.empty((S, self.N1, self.N0), dtype=torch.float32, device=self.device) if slices else None
+        rp = torch.empty((S, self.nx), dtype=torch.float32, device=self.device) if reproject else None
+        _check(lib().icon_reconstruct_stack(self._h, ctypes.byref(cfg), _ptr(stack), stack.shape[1], int(y0),
+                                            int(skip_section), _ptr(m) if slices else None,
+                                            _ptr(rp) if reproject else None, int(S), _stream()))
+        return m, rp
+
+    def reconstruct_stack_host(self, stack, y0, S, sink, iters=(0, 10, 0), data_type=1, threshold=0.03,
+                               skip_section=-1, outputs=OUT_SLICES | OUT_REPROJECTION, ny=None):
+        """icon_reconstruct_stack_host: `stack` is a device pointer (int) or a
+        CUDA tensor (sections, ny, nx); sink(s0, count, slices, reproj) gets
+        numpy views (count, N1, N0) / (count, nx) of the pinned buffers (valid
+        only during the call; None when not requested) and returns 0 to go on."""
+        import torch
+        if isinstance(stack, torch.Tensor):
+            stack = self._dev(stack, torch.float32)
+            sptr, ny = _ptr(stack), stack.shape[1]
+        else:
+            sptr = ctypes.c_void_p(int(stack))
+        N0, N1, nx = self.N0, self.N1, self.nx
+
+        def _view(p, shape):
+            if not p:
+                return None
+            n = int(np.prod(shape))
+            return np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_float)), shape=(n,)).reshape(shape)
+
+        def _cb(_ctx, s0, count, hm, hr):
+            try:
+                return int(sink(s0, count, _view(hm, (count, N1, N0)), _view(hr, (count, nx))) or 0)
+            except Exception:   # an exception cannot cross the C boundary
+                return 1
+
+        cb = BATCH_SINK(_cb)
+        a, b, c = iters
+        cfg = SolveCfg(int(a), int(b), int(c), int(data_type), float(threshold))
+        _check(lib().icon_reconstruct_stack_host(self._h, ctypes.byref(cfg), sptr, int(ny), int(y0), int(skip_section),
+                                                 int(S), int(outputs), cb, None, _stream()))
+
     TRACE_KINDS = ("xpass_fwd", "ypass_fwd", "interp_fin", "ypass_adj", "xpass_adj", "alpha", "update", "rows_fwd",
                    "layout", "row_adj")
 
@@ -258,3 +333,33 @@ class IconPlan:
 
     def launch_count(self):
         return int(lib().icon_launch_count(self._h))
+
+
+class DeviceStack:
+    """Rows y0 .. y0+S-1 of every section of a host tilt stack
+    (sections, ny, nx) uploaded in one copy (icon_stack_upload) to device
+    memory packed as (sections, S, nx); .ptr is the device address for the
+    stack calls (with ny = S, y0 = 0)."""
+
+    def __init__(self, h_stack, device=0, y0=0, S=None):
+        st = np.ascontiguousarray(h_stack, np.float32)
+        sec, ny, nx = st.shape
+        S = ny - y0 if S is None else S
+        p = ctypes.c_void_p()
+        _check(lib().icon_stack_upload(int(device), st.ctypes.data_as(ctypes.c_void_p), sec, ny, nx, int(y0), int(S),
+                                       ctypes.byref(p), None))
+        self.device, self.ptr, self.shape = int(device), p.value, (sec, S, nx)
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            lib().icon_device_free(self.device, ctypes.c_void_p(self.ptr))
+            self.ptr = None
+
+    __del__ = close
+
+
+def host_alloc(nbytes):
+    """Pinned host memory (icon_host_alloc) as a (pointer, free) pair."""
+    p = ctypes.c_void_p()
+    _check(lib().icon_host_alloc(int(nbytes), ctypes.byref(p)))
+    return p.value, lambda: lib().icon_host_free(ctypes.c_void_p(p.value))

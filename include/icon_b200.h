@@ -119,6 +119,58 @@ icon_status icon_rows_forward(icon_plan *plan, const float *d_rows, void *d_b, i
  * complexMulDoubleCU, cunfft_adjoint_2d2, complexCopyCU). */
 icon_status icon_prepare_rhs(icon_plan *plan, const float *d_rows, void *d_Ahwb, int S, void *stream);
 
+/* icon_prepare_rhs reading the rows straight from a device-resident tilt
+ * stack in file order, d_stack[sections][ny][nx] (MRC sections = tilts,
+ * y = slice): the rows of slices y0 .. y0+S-1.  With skip_section < 0 the
+ * plan's tilt i reads section i; otherwise the stack has one section more
+ * than the plan has tilts, section skip_section is left out and tilt i reads
+ * section i + (i >= skip_section) -- the cross-validation input of
+ * readSlicePart_crossV (readSlicePart_crossV.cu:3-34).  Replaces the per-row
+ * file reads of readSlicePart (readSlicePart.cu:3-31 over mrc_read_slice,
+ * mrcfile3.c:902-951, one fread per pixel) with one upload of the stack. */
+icon_status icon_prepare_rhs_stack(icon_plan *plan, const float *d_stack, int ny, int y0, int skip_section,
+                                   void *d_Ahwb, int S, void *stream);
+
+/* The per-slice pipeline of Lib_2D2 (MainCode.cu:113-142) on the device,
+ * from a tilt stack as in icon_prepare_rhs_stack to outputs in file layout:
+ * d_slices[S][N1][N0] with X fastest, the order saveMRC_real_inv writes a
+ * slice in (saveMRC_real.cu:49-53), and, when d_reproj is not NULL,
+ * d_reproj[S][nx], the reprojection at the plan's reprojection angle
+ * (icon_plan_set_reprojection).  The schedule starts from m = 0.  S may
+ * exceed the capacity (processed in chunks).  Asynchronous on `stream`. */
+icon_status icon_reconstruct_stack(icon_plan *plan, const icon_solve_cfg *cfg, const float *d_stack, int ny, int y0,
+                                   int skip_section, float *d_slices, float *d_reproj, int S, void *stream);
+
+/* icon_reconstruct_stack with the results streamed to host memory: slices
+ * y0 .. y0+S-1 in batches of the plan's capacity; each batch's outputs are
+ * copied into one of two pinned host buffers and handed to `sink` while the
+ * next batch runs on the GPU (the reference writes each slice's file after
+ * its solve, MainCode.cu:142-160, with the GPU idle meanwhile).  The sink
+ * receives the batch's first slice index (relative to y0), its slice count
+ * and the host arrays h_slices[count][N1][N0] (X fastest) and
+ * h_reproj[count][nx] -- NULL unless requested in `outputs` -- which stay
+ * valid until it returns; a nonzero return stops the run with an error.
+ * The sink runs on the calling thread.  Returns after the last batch's sink. */
+#define ICON_OUT_SLICES 1
+#define ICON_OUT_REPROJECTION 2
+typedef int (*icon_batch_sink)(void *ctx, int s0, int count, const float *h_slices, const float *h_reproj);
+icon_status icon_reconstruct_stack_host(icon_plan *plan, const icon_solve_cfg *cfg, const float *d_stack, int ny,
+                                        int y0, int skip_section, int S, int outputs, icon_batch_sink sink, void *ctx,
+                                        void *stream);
+
+/* Pinned (page-locked, portable) host memory for a stack read from a file,
+ * so that icon_stack_upload copies at full speed, and its release. */
+icon_status icon_host_alloc(size_t bytes, void **out);
+icon_status icon_host_free(void *h_ptr);
+
+/* One upload of the rows y0 .. y0+S-1 of every section of a host tilt stack
+ * h_stack[sections][ny][nx] (file order) to new device memory on `device`,
+ * packed as d_stack[sections][S][nx] (so ny = S, y0 = 0 in the stack calls).
+ * A single 2-D copy; synchronises `stream`.  Free with icon_device_free. */
+icon_status icon_stack_upload(int device, const float *h_stack, int sections, int ny, int nx, int y0, int S,
+                              float **d_stack, void *stream);
+icon_status icon_device_free(int device, void *d_ptr);
+
 /* ICON iterations on S slices: replaces Iteration3 (Iteration2.cu:3-150)
  * with Alpha2 (alpha_new2.cu:3-119).  d_m is the start value when
  * warm_start != 0 and is zeroed first otherwise (Iteration2.cu:33); it
