@@ -278,12 +278,6 @@ enum Kind { K_XF = 0, K_YF, K_FIN, K_YA, K_XA, K_ALPHA, K_UPD, K_ROWS, K_LAYOUT,
     default: { using L = icon::Launch<8>; __VA_ARGS__; } break;          \
     }
 
-// Shared-memory bytes of a rotated y-pass row buffer.
-inline size_t ybuf_bytes(int n1, int B)
-{
-    int sb = B == 8 ? 10 : (B == 4 ? 6 : B);
-    return (size_t)(n1 + 2 * icon::kHalo) * sb * sizeof(float2);
-}
 
 struct DeviceGuard {
     int prev = -1;
@@ -652,7 +646,7 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
     p->thr_x = p->n0 * B / p->ex;
     p->thr_y = p->n1 * B / p->ey;
     p->smem_x = (size_t)p->n0 * B * sizeof(float2);
-    p->smem_y = ybuf_bytes(p->n1, B) + icon::ypass_fwd_pre_bytes();
+    p->smem_y = icon::ypass_fwd_smem(p->n1, B);
     p->smem_ya = icon::ypass_adj_smem(p->n1, B);
     int smem_max = 0;
     ICON_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));

@@ -261,14 +261,28 @@ __device__ __forceinline__ void dft_inplace(float2 (&a)[R], float dir)
     if constexpr (R >= 2) dft_stage<R, 2>(a, dir);
 }
 
+// Position of point p in the intermediate buffer s.  With SWZ, points p and
+// p ^ 1 trade places when bit zs of p is set (zs = log2 of the first pass's
+// radix).  The first pass writes points j*R + r, so with an unpadded stride
+// of 64 bytes (SB = B = 8) the four butterflies j of a warp would all land on
+// the same 16 banks; the swap puts two of them on the other 16, and the
+// contiguous accesses of the later passes keep two even and two odd rows per
+// warp, so every 8-byte access of the FFT is conflict-free.
+template <bool SWZ>
+__device__ __forceinline__ int swz_pos(int p, int zs)
+{
+    if constexpr (SWZ) return p ^ ((p >> zs) & 1);
+    else return p;
+}
+
 // One Stockham pass of radix R over n points for B slices, E values per
 // thread (E/R butterflies).  FIRST: inputs come from ld(pos, b) instead of
 // s[pos*SB + b]; LAST: outputs go to st(pos, b, value) instead of s.  A
 // barrier separates the reads of a pass from its writes, so ld may read s
 // and st may write s; the caller syncs after a LAST pass if st wrote s.
-template <int R, int B, int SB, int E, bool FIRST, bool LAST, bool GUARD, class Ld, class St>
+template <int R, int B, int SB, int E, bool FIRST, bool LAST, bool GUARD, bool SWZ, class Ld, class St>
 __device__ __forceinline__ void fpass(float2 *s, int n, int Ns, const float2 *__restrict__ tw, float dir, Ld &ld, St &st,
-                                      int T)
+                                      int T, int zs)
 {
     constexpr int Q = E / R;
     constexpr int LB = Log2B<B>::v;
@@ -294,7 +308,7 @@ __device__ __forceinline__ void fpass(float2 *s, int n, int Ns, const float2 *__
             for (int r = 0; r < R; ++r) {
                 float2 x;
                 if constexpr (FIRST) x = ld(j + r * nb, b);
-                else x = s[(j + r * nb) * SB + b];
+                else x = s[swz_pos<SWZ>(j + r * nb, zs) * SB + b];
                 if (!FIRST && r > 0 && Ns > 1) {
                     if ((r & 7) == 0) {
                         w = __ldg(&tw[r * k * step]);
@@ -320,23 +334,23 @@ __device__ __forceinline__ void fpass(float2 *s, int n, int Ns, const float2 *__
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if constexpr (LAST) st(base + r * Ns, b, v[q][r]);
-                else s[(base + r * Ns) * SB + b] = v[q][r];
+                else s[swz_pos<SWZ>(base + r * Ns, zs) * SB + b] = v[q][r];
             }
         }
     }
     if constexpr (!LAST) __syncthreads();
 }
 
-template <int R, int B, int SB, int E, bool GUARD, class Ld, class St>
+template <int R, int B, int SB, int E, bool GUARD, bool SWZ, class Ld, class St>
 __device__ __forceinline__ void fpass_any(bool first, bool last, float2 *s, int n, int Ns, const float2 *tw, float dir,
-                                          Ld &ld, St &st, int T)
+                                          Ld &ld, St &st, int T, int zs)
 {
     if (first) {
-        if (last) fpass<R, B, SB, E, true, true, GUARD>(s, n, Ns, tw, dir, ld, st, T);
-        else fpass<R, B, SB, E, true, false, GUARD>(s, n, Ns, tw, dir, ld, st, T);
+        if (last) fpass<R, B, SB, E, true, true, GUARD, SWZ>(s, n, Ns, tw, dir, ld, st, T, zs);
+        else fpass<R, B, SB, E, true, false, GUARD, SWZ>(s, n, Ns, tw, dir, ld, st, T, zs);
     } else {
-        if (last) fpass<R, B, SB, E, false, true, GUARD>(s, n, Ns, tw, dir, ld, st, T);
-        else fpass<R, B, SB, E, false, false, GUARD>(s, n, Ns, tw, dir, ld, st, T);
+        if (last) fpass<R, B, SB, E, false, true, GUARD, SWZ>(s, n, Ns, tw, dir, ld, st, T, zs);
+        else fpass<R, B, SB, E, false, false, GUARD, SWZ>(s, n, Ns, tw, dir, ld, st, T, zs);
     }
 }
 
@@ -344,24 +358,26 @@ __device__ __forceinline__ void fpass_any(bool first, bool last, float2 *s, int 
 // first n*B/E threads of the block: blockDim.x == n*B/E unless GUARD, in which
 // case extra threads only take part in the barriers.  The first pass reads ld(pos, b) (natural order), the last pass
 // hands st(pos, b, value) the outputs in natural order; intermediate passes
-// use s[n][SB].  The first pass has no twiddles (Ns = 1).  E is 16 or 32:
-// passes of radix E after one pass of radix 2^(lg mod log2 E).
-template <int B, int SB, int E, bool GUARD = false, class Ld, class St>
+// use s[n][SB] (positions permuted by swz_pos<SWZ>).  The first pass has no
+// twiddles (Ns = 1).  E is 16 or 32: passes of radix E after one pass of
+// radix 2^(lg mod log2 E).
+template <int B, int SB, int E, bool GUARD = false, bool SWZ = false, class Ld, class St>
 __device__ __forceinline__ void fft_fused(float2 *s, int n, int lg, const float2 *__restrict__ tw, float dir, Ld &ld, St &st)
 {
     constexpr int LE = (E == 32) ? 5 : 4;
     const int T = n * B / E;
     const int rem = lg % LE;
+    const int zs = rem ? rem : LE;   // log2 of the first pass's radix
     int Ns = 1;
     bool first = true;
     if (rem) {
         bool last = (1 << rem) == n;
         switch (rem) {
-        case 1: fpass_any<2, B, SB, E, GUARD>(first, last, s, n, Ns, tw, dir, ld, st, T); break;
-        case 2: fpass_any<4, B, SB, E, GUARD>(first, last, s, n, Ns, tw, dir, ld, st, T); break;
-        case 3: fpass_any<8, B, SB, E, GUARD>(first, last, s, n, Ns, tw, dir, ld, st, T); break;
+        case 1: fpass_any<2, B, SB, E, GUARD, SWZ>(first, last, s, n, Ns, tw, dir, ld, st, T, zs); break;
+        case 2: fpass_any<4, B, SB, E, GUARD, SWZ>(first, last, s, n, Ns, tw, dir, ld, st, T, zs); break;
+        case 3: fpass_any<8, B, SB, E, GUARD, SWZ>(first, last, s, n, Ns, tw, dir, ld, st, T, zs); break;
         default:
-            if constexpr (E == 32) fpass_any<16, B, SB, E, GUARD>(first, last, s, n, Ns, tw, dir, ld, st, T);
+            if constexpr (E == 32) fpass_any<16, B, SB, E, GUARD, SWZ>(first, last, s, n, Ns, tw, dir, ld, st, T, zs);
             break;
         }
         Ns = 1 << rem;
@@ -369,7 +385,7 @@ __device__ __forceinline__ void fft_fused(float2 *s, int n, int lg, const float2
     }
     while (Ns < n) {
         bool last = Ns * E == n;
-        fpass_any<E, B, SB, E, GUARD>(first, last, s, n, Ns, tw, dir, ld, st, T);
+        fpass_any<E, B, SB, E, GUARD, SWZ>(first, last, s, n, Ns, tw, dir, ld, st, T, zs);
         Ns *= E;
         first = false;
     }

@@ -202,6 +202,19 @@ constexpr int kPreEntries = 256;
 constexpr int kPreRecord = kLdPhiy * 4 + 8;
 __host__ __device__ inline size_t ypass_fwd_pre_bytes() { return (size_t)kPreEntries * kPreRecord; }
 
+// Row stride (float2) of k_ypass_fwd's rotated row buffer: unpadded for
+// B = 8 (64-byte rows; the interpolation reads pairs of rows as 128-byte
+// blocks, conflict-free), the padded RowStride otherwise.
+template <int B>
+struct YfStride {
+    static constexpr int v = (B == 8) ? 8 : RowStride<B>::v;
+};
+__host__ __device__ inline size_t ypass_fwd_smem(int n1, int B)
+{
+    size_t sb = (B == 8) ? 8 : (B == 4) ? 6 : B;
+    return (size_t)(n1 + 2 * kHalo) * sb * sizeof(float2) + ypass_fwd_pre_bytes();
+}
+
 // Forward y-pass fused with the y-direction interpolation.  Row x of G1 holds
 // the N1 nonzero columns; column Y sits at y with (y + N1/2) % n1 == Y.
 // P[G][M][14][B]: P[j][t0] = sum_t1 phiy[j][t1] * G[x][(iy0_j + t1) mod n1],
@@ -214,7 +227,8 @@ template <int B, int E>
 __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, float2 *__restrict__ P)
 {
     extern __shared__ float2 s[];
-    constexpr int SB = RowStride<B>::v;
+    constexpr int SB = YfStride<B>::v;
+    constexpr bool kPairs = (B == 8);   // 64-byte rows read as 128-byte row pairs
     const int grp = blockIdx.x, x = blockIdx.y, n = g.n1, N1 = g.N1;
     const int T = blockDim.x;
     const float2 *rowin = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
@@ -246,7 +260,7 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
         return (y & 1) ? make_float2(-v.x, -v.y) : v;      // rotates the output by n/2
     };
     auto st = [=](int q, int b, float2 v) { row[q * SB + b] = v; };
-    fft_fused<B, SB, E>(row, n, g.lg1, g.tw1, -1.f, ld, st);
+    fft_fused<B, SB, E, false, kPairs>(row, n, g.lg1, g.tw1, -1.f, ld, st);
     cp_async_wait<0>();
     __syncthreads();
     fill_halo<B, SB>(s, n);
@@ -288,20 +302,55 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
             py[4 * q + 2] = cur.py[q].z;
             py[4 * q + 3] = cur.py[q].w;
         }
-        float2 acc[B];
+        if constexpr (kPairs) {
+            // Taps 2p and 2p+1 are rows r and r+1, one 128-byte block = eight
+            // 16-byte chunks (chunk c: row r + c/4, slices 2(c%4), 2(c%4)+1),
+            // whose bank slots are (4r + c) % 8.  At step k lane l reads the
+            // chunk in slot (l + k) % 8, so the eight lanes of each quarter
+            // warp hit eight different slots: no bank conflicts, whatever the
+            // rows of the lanes' entries.  acc[k % 4] then always holds the
+            // slices of quad (l + k) % 4.
+            const int lane8 = threadIdx.x & 7;
+            const int r0 = cur.iy + rofs;
+            const char *rb = reinterpret_cast<const char *>(s) + (size_t)r0 * (SB * sizeof(float2));
+            const int o = lane8 + ((r0 & 1) << 2);
+            float4 acc[4];
 #pragma unroll
-        for (int b = 0; b < B; ++b) acc[b] = make_float2(0.f, 0.f);
+            for (int k = 0; k < 4; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int t1 = 0; t1 < kTaps; ++t1) {
-            float2 v[B];
-            load_b<B>(sr + t1 * SB, v);
+            for (int pr = 0; pr < kTaps / 2; ++pr) {
+                const float wa = py[2 * pr], wb = py[2 * pr + 1];
 #pragma unroll
-            for (int b = 0; b < B; ++b) {
-                acc[b].x = fmaf(v[b].x, py[t1], acc[b].x);
-                acc[b].y = fmaf(v[b].y, py[t1], acc[b].y);
+                for (int k = 0; k < 8; ++k) {
+                    const int c = (o + k) & 7;
+                    const float4 v = *reinterpret_cast<const float4 *>(rb + pr * 128 + c * 16);
+                    const float w = (c & 4) ? wb : wa;
+                    float4 &a = acc[k & 3];
+                    a.x = fmaf(v.x, w, a.x);
+                    a.y = fmaf(v.y, w, a.y);
+                    a.z = fmaf(v.z, w, a.z);
+                    a.w = fmaf(v.w, w, a.w);
+                }
             }
+            float4 *dst = reinterpret_cast<float4 *>(P + pbase + ((size_t)j * kTaps + t0) * B);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) dst[(lane8 + k) & 3] = acc[k];
+        } else {
+            float2 acc[B];
+#pragma unroll
+            for (int b = 0; b < B; ++b) acc[b] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int t1 = 0; t1 < kTaps; ++t1) {
+                float2 v[B];
+                load_b<B>(sr + t1 * SB, v);
+#pragma unroll
+                for (int b = 0; b < B; ++b) {
+                    acc[b].x = fmaf(v[b].x, py[t1], acc[b].x);
+                    acc[b].y = fmaf(v[b].y, py[t1], acc[b].y);
+                }
+            }
+            store_b<B>(P + pbase + ((size_t)j * kTaps + t0) * B, acc);
         }
-        store_b<B>(P + pbase + ((size_t)j * kTaps + t0) * B, acc);
         cur = nxt;
         i = i2;
     }
