@@ -325,11 +325,11 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
                     const int c = (o + k) & 7;
                     const float4 v = *reinterpret_cast<const float4 *>(rb + pr * 128 + c * 16);
                     const float w = (c & 4) ? wb : wa;
+                    const float2 ww = make_float2(w, w);
                     float4 &a = acc[k & 3];
-                    a.x = fmaf(v.x, w, a.x);
-                    a.y = fmaf(v.y, w, a.y);
-                    a.z = fmaf(v.z, w, a.z);
-                    a.w = fmaf(v.w, w, a.w);
+                    const float2 lo = fma2(make_float2(v.x, v.y), ww, make_float2(a.x, a.y));
+                    const float2 hi = fma2(make_float2(v.z, v.w), ww, make_float2(a.z, a.w));
+                    a = make_float4(lo.x, lo.y, hi.x, hi.y);
                 }
             }
             float4 *dst = reinterpret_cast<float4 *>(P + pbase + ((size_t)j * kTaps + t0) * B);
@@ -471,12 +471,11 @@ __device__ __forceinline__ void gather_rows(int i0, int r0ofs, const unsigned sh
         float2 q[B];
         load_b<B>(Qs + e * SB, q);
 #pragma unroll
-        for (int k = 0; k < R; ++k)
+        for (int k = 0; k < R; ++k) {
+            const float2 pp = make_float2(p[k], p[k]);
 #pragma unroll
-            for (int b = 0; b < B; ++b) {
-                acc[k][b].x = fmaf(q[b].x, p[k], acc[k][b].x);
-                acc[k][b].y = fmaf(q[b].y, p[k], acc[k][b].y);
-            }
+            for (int b = 0; b < B; ++b) acc[k][b] = fma2(q[b], pp, acc[k][b]);
+        }
     }
 }
 
