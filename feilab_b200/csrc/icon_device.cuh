@@ -22,6 +22,27 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 }
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 
+// a + b and a - b on both components with one packed Blackwell instruction
+// (add/sub.rn.f32x2): the same rounding as two scalar adds.
+__device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b)
+{
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
 // a * b + c on both components with one packed Blackwell instruction
 // (fma.rn.f32x2); each component is rounded exactly as fmaf rounds it.
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
@@ -258,8 +279,8 @@ __device__ __forceinline__ void dft_stage(float2 (&a)[R], float dir)
         for (int k = 0; k < LEN / 2; ++k) {
             float2 o = a[i + k + LEN / 2];
             float2 t = (k == 0) ? o : cmul(w32((k * (32 / LEN)) & 31, dir), o);
-            a[i + k + LEN / 2] = csub(a[i + k], t);
-            a[i + k] = cadd(a[i + k], t);
+            a[i + k + LEN / 2] = sub2(a[i + k], t);
+            a[i + k] = add2(a[i + k], t);
         }
     }
     if constexpr (LEN < R) dft_stage<R, 2 * LEN>(a, dir);
