@@ -537,11 +537,18 @@ __global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, f
         }
         cp_async_commit();
     };
-    float2 acc[R][1][B];                  // gather_rows<..., 1> takes one row as [1][B]
+    // Thread t owns NS strips of RS consecutive rows, strip t + k*T starting
+    // at row RS*(t + k*T); one gather of a strip loads each covering entry
+    // once for its RS rows.
+    constexpr int RS = (B == 8 && R % 2 == 0) ? 2 : 1;
+    constexpr int NS = R / RS;
+    float2 acc[NS][RS][B];
 #pragma unroll
-    for (int k = 0; k < R; ++k)
+    for (int k = 0; k < NS; ++k)
 #pragma unroll
-        for (int b = 0; b < B; ++b) acc[k][0][b] = make_float2(0.f, 0.f);
+        for (int j = 0; j < RS; ++j)
+#pragma unroll
+            for (int b = 0; b < B; ++b) acc[k][j][b] = make_float2(0.f, 0.f);
     if (nch > 0) {
         copy_async(lb, g.ent_lb + (size_t)x * ldl, (size_t)ldl * sizeof(unsigned short));
         issue(0);
@@ -555,21 +562,25 @@ __global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, f
         const float *Ps = bufP(c);
         const int *Rs = bufR(c);
 #pragma unroll
-        for (int k = 0; k < R; ++k) {
-            const int r = threadIdx.x + k * T;
+        for (int k = 0; k < NS; ++k) {
+            const int r = RS * (threadIdx.x + k * T);
             if (r < n) {
-                gather_rows<B, SB, 1>(r + kHalo, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
-                // Rows 0..7 and n-8..n-1 also take the halo rows that alias them.
-                if (r < kHalo) gather_rows<B, SB, 1>(r + kHalo + n, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
-                if (r >= n - kHalo) gather_rows<B, SB, 1>(r + kHalo - n, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
+                gather_rows<B, SB, RS>(r + kHalo, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
+                // Rows 0..7 and n-8..n-1 also take the halo rows that alias
+                // them (kHalo is a multiple of RS, so no strip straddles).
+                if (r < kHalo) gather_rows<B, SB, RS>(r + kHalo + n, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
+                if (r >= n - kHalo) gather_rows<B, SB, RS>(r + kHalo - n, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
             }
         }
     }
     __syncthreads();                      // the row buffer reuses the chunk buffers
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int r = threadIdx.x + k * T;
-        if (r < n) store_b<B>(s + (size_t)r * SB, acc[k][0]);
+    for (int k = 0; k < NS; ++k) {
+        const int r = RS * (threadIdx.x + k * T);
+        if (r < n) {
+#pragma unroll
+            for (int j = 0; j < RS; ++j) store_b<B>(s + (size_t)(r + j) * SB, acc[k][j]);
+        }
     }
     __syncthreads();
     float2 *row = s;
