@@ -422,7 +422,7 @@ __device__ __forceinline__ int lower_bound_s(const int *key, int lo, int hi, int
 // Entries of a row staged at a time by the adjoint gather, and the padded
 // stride of a staged phiy window (so that neighbouring windows fall in
 // different shared-memory banks).
-constexpr int kChunk = 192;
+constexpr int kChunk = 320;
 constexpr int kLdPs = 20;
 
 // Entries of grid row x whose first y tap r0 (in the rotated buffer with a
