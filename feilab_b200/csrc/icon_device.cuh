@@ -314,8 +314,8 @@ __device__ __forceinline__ int swz_pos(int p, int zs)
 // s[pos*SB + b]; LAST: outputs go to st(pos, b, value) instead of s.  A
 // barrier separates the reads of a pass from its writes, so ld may read s
 // and st may write s; the caller syncs after a LAST pass if st wrote s.
-template <int R, int B, int SB, int E, bool FIRST, bool LAST, bool GUARD, bool SWZ, class Ld, class St>
-__device__ __forceinline__ void fpass(float2 *s, int n, int Ns, const float2 *__restrict__ tw, float dir, Ld &ld, St &st,
+template <int R, int B, int SB, int E, bool FIRST, bool LAST, bool GUARD, bool SWZ, bool TWS, class Ld, class St>
+__device__ __forceinline__ void fpass(float2 *s, int n, int Ns, const float2 *tw, float dir, Ld &ld, St &st,
                                       int T, int zs)
 {
     constexpr int Q = E / R;
@@ -333,8 +333,10 @@ __device__ __forceinline__ void fpass(float2 *s, int n, int Ns, const float2 *__
             // Inter-pass twiddle w^(r k step), w = exp(-dir 2 pi i / n): read
             // from the table for r = 0, 8, 16, 24 and stepped by w^(k step)
             // in between (at most 7 products from a table value).
+            // With TWS the table is in shared memory and every twiddle is
+            // read from it (r k step < n).
             float2 w1 = make_float2(1.f, 0.f), w = w1;
-            if (!FIRST && Ns > 1) {
+            if (!TWS && !FIRST && Ns > 1) {
                 w1 = __ldg(&tw[k * step]);
                 w1.y = -dir * w1.y;
             }
@@ -343,7 +345,11 @@ __device__ __forceinline__ void fpass(float2 *s, int n, int Ns, const float2 *__
                 float2 x;
                 if constexpr (FIRST) x = ld(j + r * nb, b);
                 else x = s[swz_pos<SWZ>(j + r * nb, zs) * SB + b];
-                if (!FIRST && r > 0 && Ns > 1) {
+                if (TWS && !FIRST && r > 0 && Ns > 1) {
+                    w = tw[r * k * step];
+                    w.y = -dir * w.y;
+                    x = cmul(x, w);
+                } else if (!FIRST && r > 0 && Ns > 1) {
                     if ((r & 7) == 0) {
                         w = __ldg(&tw[r * k * step]);
                         w.y = -dir * w.y;
@@ -375,16 +381,16 @@ __device__ __forceinline__ void fpass(float2 *s, int n, int Ns, const float2 *__
     if constexpr (!LAST) __syncthreads();
 }
 
-template <int R, int B, int SB, int E, bool GUARD, bool SWZ, class Ld, class St>
+template <int R, int B, int SB, int E, bool GUARD, bool SWZ, bool TWS, class Ld, class St>
 __device__ __forceinline__ void fpass_any(bool first, bool last, float2 *s, int n, int Ns, const float2 *tw, float dir,
                                           Ld &ld, St &st, int T, int zs)
 {
     if (first) {
-        if (last) fpass<R, B, SB, E, true, true, GUARD, SWZ>(s, n, Ns, tw, dir, ld, st, T, zs);
-        else fpass<R, B, SB, E, true, false, GUARD, SWZ>(s, n, Ns, tw, dir, ld, st, T, zs);
+        if (last) fpass<R, B, SB, E, true, true, GUARD, SWZ, TWS>(s, n, Ns, tw, dir, ld, st, T, zs);
+        else fpass<R, B, SB, E, true, false, GUARD, SWZ, TWS>(s, n, Ns, tw, dir, ld, st, T, zs);
     } else {
-        if (last) fpass<R, B, SB, E, false, true, GUARD, SWZ>(s, n, Ns, tw, dir, ld, st, T, zs);
-        else fpass<R, B, SB, E, false, false, GUARD, SWZ>(s, n, Ns, tw, dir, ld, st, T, zs);
+        if (last) fpass<R, B, SB, E, false, true, GUARD, SWZ, TWS>(s, n, Ns, tw, dir, ld, st, T, zs);
+        else fpass<R, B, SB, E, false, false, GUARD, SWZ, TWS>(s, n, Ns, tw, dir, ld, st, T, zs);
     }
 }
 
@@ -395,8 +401,10 @@ __device__ __forceinline__ void fpass_any(bool first, bool last, float2 *s, int 
 // use s[n][SB] (positions permuted by swz_pos<SWZ>).  The first pass has no
 // twiddles (Ns = 1).  E is 16 or 32: passes of radix E after one pass of
 // radix 2^(lg mod log2 E).
-template <int B, int SB, int E, bool GUARD = false, bool SWZ = false, class Ld, class St>
-__device__ __forceinline__ void fft_fused(float2 *s, int n, int lg, const float2 *__restrict__ tw, float dir, Ld &ld, St &st)
+// TWS: tw is a copy of the table in shared memory (every twiddle read from
+// it); otherwise tw is global and twiddles between table reads are products.
+template <int B, int SB, int E, bool GUARD = false, bool SWZ = false, bool TWS = false, class Ld, class St>
+__device__ __forceinline__ void fft_fused(float2 *s, int n, int lg, const float2 *tw, float dir, Ld &ld, St &st)
 {
     constexpr int LE = (E == 32) ? 5 : 4;
     const int T = n * B / E;
@@ -407,11 +415,11 @@ __device__ __forceinline__ void fft_fused(float2 *s, int n, int lg, const float2
     if (rem) {
         bool last = (1 << rem) == n;
         switch (rem) {
-        case 1: fpass_any<2, B, SB, E, GUARD, SWZ>(first, last, s, n, Ns, tw, dir, ld, st, T, zs); break;
-        case 2: fpass_any<4, B, SB, E, GUARD, SWZ>(first, last, s, n, Ns, tw, dir, ld, st, T, zs); break;
-        case 3: fpass_any<8, B, SB, E, GUARD, SWZ>(first, last, s, n, Ns, tw, dir, ld, st, T, zs); break;
+        case 1: fpass_any<2, B, SB, E, GUARD, SWZ, TWS>(first, last, s, n, Ns, tw, dir, ld, st, T, zs); break;
+        case 2: fpass_any<4, B, SB, E, GUARD, SWZ, TWS>(first, last, s, n, Ns, tw, dir, ld, st, T, zs); break;
+        case 3: fpass_any<8, B, SB, E, GUARD, SWZ, TWS>(first, last, s, n, Ns, tw, dir, ld, st, T, zs); break;
         default:
-            if constexpr (E == 32) fpass_any<16, B, SB, E, GUARD, SWZ>(first, last, s, n, Ns, tw, dir, ld, st, T, zs);
+            if constexpr (E == 32) fpass_any<16, B, SB, E, GUARD, SWZ, TWS>(first, last, s, n, Ns, tw, dir, ld, st, T, zs);
             break;
         }
         Ns = 1 << rem;
@@ -419,7 +427,7 @@ __device__ __forceinline__ void fft_fused(float2 *s, int n, int lg, const float2
     }
     while (Ns < n) {
         bool last = Ns * E == n;
-        fpass_any<E, B, SB, E, GUARD, SWZ>(first, last, s, n, Ns, tw, dir, ld, st, T, zs);
+        fpass_any<E, B, SB, E, GUARD, SWZ, TWS>(first, last, s, n, Ns, tw, dir, ld, st, T, zs);
         Ns *= E;
         first = false;
     }

@@ -202,6 +202,12 @@ constexpr int kPreEntries = 256;
 constexpr int kPreRecord = kLdPhiy * 4 + 8;
 __host__ __device__ inline size_t ypass_fwd_pre_bytes() { return (size_t)kPreEntries * kPreRecord; }
 
+// The y-passes copy the FFT's twiddle table (n1 float2) into shared memory
+// when it fits beside their buffers (n1 <= 2048); longer rows read it from
+// global memory.
+__host__ __device__ inline bool ypass_tw_shared(int n1) { return n1 <= 2048; }
+__host__ __device__ inline size_t ypass_tw_bytes(int n1) { return ypass_tw_shared(n1) ? (size_t)n1 * 8 : 0; }
+
 // Row stride (float2) of k_ypass_fwd's rotated row buffer: unpadded for
 // B = 8 (64-byte rows; the interpolation reads pairs of rows as 128-byte
 // blocks, conflict-free), the padded RowStride otherwise.
@@ -212,7 +218,7 @@ struct YfStride {
 __host__ __device__ inline size_t ypass_fwd_smem(int n1, int B)
 {
     size_t sb = (B == 8) ? 8 : (B == 4) ? 6 : B;
-    return (size_t)(n1 + 2 * kHalo) * sb * sizeof(float2) + ypass_fwd_pre_bytes();
+    return (size_t)(n1 + 2 * kHalo) * sb * sizeof(float2) + ypass_fwd_pre_bytes() + ypass_tw_bytes(n1);
 }
 
 // Forward y-pass fused with the y-direction interpolation.  Row x of G1 holds
@@ -236,10 +242,14 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
     float *pre_phi = reinterpret_cast<float *>(s + (size_t)(n + 2 * kHalo) * SB);   // [kPreEntries][16]
     int *pre_jt = reinterpret_cast<int *>(pre_phi + kPreEntries * kLdPhiy);           // [kPreEntries]
     int *pre_iy = pre_jt + kPreEntries;                                                 // [kPreEntries]
+    float2 *tw_s = reinterpret_cast<float2 *>(pre_iy + kPreEntries);                    // [n] twiddles
+    const float2 *tws = ypass_tw_shared(n) ? tw_s : g.tw1;
     const int e0 = g.row_off[x], cnt = g.row_off[x + 1] - e0;
     const int staged = min(cnt, min(T, kPreEntries));
-    // Group 1: the N1 nonzero values of the row (contiguous in G1).
+    // Group 1: the N1 nonzero values of the row (contiguous in G1) and the
+    // FFT's twiddle table.
     copy_async(row, rowin, (size_t)N1 * B * sizeof(float2));
+    if (ypass_tw_shared(n)) copy_async(tw_s, g.tw1, (size_t)n * sizeof(float2));
     cp_async_commit();
     // Group 2: tables of the first entries.
     if ((int)threadIdx.x < staged) {
@@ -260,7 +270,7 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
         return (y & 1) ? make_float2(-v.x, -v.y) : v;      // rotates the output by n/2
     };
     auto st = [=](int q, int b, float2 v) { row[q * SB + b] = v; };
-    fft_fused<B, SB, E, false, kPairs>(row, n, g.lg1, g.tw1, -1.f, ld, st);
+    fft_fused<B, SB, E, false, kPairs, true>(row, n, g.lg1, tws, -1.f, ld, st);
     cp_async_wait<0>();
     __syncthreads();
     fill_halo<B, SB>(s, n);
@@ -422,7 +432,7 @@ __device__ __forceinline__ int lower_bound_s(const int *key, int lo, int hi, int
 // Entries of a row staged at a time by the adjoint gather, and the padded
 // stride of a staged phiy window (so that neighbouring windows fall in
 // different shared-memory banks).
-constexpr int kChunk = 320;
+constexpr int kChunk = 304;
 constexpr int kLdPs = 20;
 
 // Entries of grid row x whose first y tap r0 (in the rotated buffer with a
@@ -440,12 +450,17 @@ __host__ __device__ inline size_t ypass_adj_chunk_bytes(int B)
     size_t sb = (B == 8) ? 10 : (B == 4) ? 6 : B;
     return (size_t)kChunk * (sb * sizeof(float2) + kLdPs * sizeof(float) + sizeof(int));
 }
-__host__ __device__ inline size_t ypass_adj_smem(int n1, int B)
+__host__ __device__ inline size_t ypass_adj_region(int n1, int B)
 {
     size_t sb = (B == 8) ? 10 : (B == 4) ? 6 : B;
     size_t row = (size_t)n1 * sb * sizeof(float2);
     size_t gather = 2 * ypass_adj_chunk_bytes(B) + (((size_t)lb_ld(n1) * sizeof(unsigned short) + 15) & ~(size_t)15);
     return row > gather ? row : gather;
+}
+// The region above plus the FFT's twiddle table behind it.
+__host__ __device__ inline size_t ypass_adj_smem(int n1, int B)
+{
+    return ypass_adj_region(n1, B) + ypass_tw_bytes(n1);
 }
 
 // Adds the staged entries covering buffer rows i0 .. i0+R-1 (r0 in
@@ -549,6 +564,10 @@ __global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, f
         for (int j = 0; j < RS; ++j)
 #pragma unroll
             for (int b = 0; b < B; ++b) acc[k][j][b] = make_float2(0.f, 0.f);
+    float2 *tw_s = reinterpret_cast<float2 *>(base + ypass_adj_region(n, B));   // [n] twiddles
+    const float2 *tws = ypass_tw_shared(n) ? tw_s : g.tw1;
+    if (ypass_tw_shared(n)) copy_async(tw_s, g.tw1, (size_t)n * sizeof(float2));
+    cp_async_commit();
     if (nch > 0) {
         copy_async(lb, g.ent_lb + (size_t)x * ldl, (size_t)ldl * sizeof(unsigned short));
         issue(0);
@@ -573,6 +592,7 @@ __global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, f
             }
         }
     }
+    cp_async_wait<0>();                   // the twiddles (rows without entries wait here)
     __syncthreads();                      // the row buffer reuses the chunk buffers
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
@@ -590,7 +610,7 @@ __global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, f
         int Y = (kq + N1 / 2) & (n - 1);
         if (Y < N1) out[(size_t)Y * B + b] = (kq & 1) ? make_float2(-v.x, -v.y) : v;   // undoes the rotation
     };
-    fft_fused<B, SB, E, GUARD>(row, n, g.lg1, g.tw1, +1.f, ld, st);
+    fft_fused<B, SB, E, GUARD, false, true>(row, n, g.lg1, tws, +1.f, ld, st);
 }
 
 // -------------------------------------------------------------- K1T ----
