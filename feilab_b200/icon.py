@@ -115,6 +115,7 @@ class IconPlan:
         g = Geometry(int(nx), int(thickness), len(self.tilts),
                      self.tilts.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(capacity), int(device))
         h = ctypes.c_void_p()
+        self._destroy = lib().icon_plan_destroy     # held so that __del__ works at interpreter exit
         _check(lib().icon_plan_create(ctypes.byref(g), ctypes.byref(h)))
         self._h = h
         d = (ctypes.c_int * 10)()
@@ -125,7 +126,7 @@ class IconPlan:
     def close(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            lib().icon_plan_destroy(h)
+            self._destroy(h)
             self._h = None
 
     __del__ = close
@@ -346,13 +347,14 @@ class DeviceStack:
         sec, ny, nx = st.shape
         S = ny - y0 if S is None else S
         p = ctypes.c_void_p()
+        self._free = lib().icon_device_free
         _check(lib().icon_stack_upload(int(device), st.ctypes.data_as(ctypes.c_void_p), sec, ny, nx, int(y0), int(S),
                                        ctypes.byref(p), None))
         self.device, self.ptr, self.shape = int(device), p.value, (sec, S, nx)
 
     def close(self):
         if getattr(self, "ptr", None):
-            lib().icon_device_free(self.device, ctypes.c_void_p(self.ptr))
+            self._free(self.device, ctypes.c_void_p(self.ptr))
             self.ptr = None
 
     __del__ = close

@@ -84,6 +84,7 @@ class Mask:
     def __init__(self, n, tilts, rate05, rate03, explicit, gauss_width=None, capacity=16):
         t = np.ascontiguousarray(np.asarray(tilts, np.float32))
         h = ctypes.c_void_p()
+        self._destroy = _mask_lib().icon_mask_destroy     # held so that __del__ works at interpreter exit
         _check(_mask_lib().icon_mask_create(int(n), t.ctypes.data_as(ctypes.c_void_p), t.size, float(rate05),
                                             float(rate03), int(explicit), int(gauss_width or 0), int(capacity),
                                             ctypes.byref(h)))
@@ -91,7 +92,7 @@ class Mask:
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
-            _mask_lib().icon_mask_destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     __del__ = close

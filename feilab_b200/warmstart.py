@@ -101,6 +101,7 @@ class Network:
         self.plan = plan
         self.capacity = int(capacity or plan.capacity)
         h = ctypes.c_void_p()
+        self._destroy = lib().icon_ws_destroy     # held so that __del__ works at interpreter exit
         with torch.cuda.device(plan.device):
             _check(lib().icon_ws_create(plan._h, self.capacity, ctypes.byref(h)))
         self._h = h
@@ -109,7 +110,7 @@ class Network:
     def close(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            lib().icon_ws_destroy(h)
+            self._destroy(h)
             self._h = None
 
     __del__ = close
