@@ -189,6 +189,8 @@ struct icon_plan {
     float *m = nullptr, *rows = nullptr, *outrp = nullptr, *mout = nullptr;
     double *part_rtr = nullptr, *part_rtar = nullptr, *alpha = nullptr;
     double *step_part = nullptr, *step = nullptr;   // relative update size (icon_solve_until)
+    float *wgroup = nullptr;   // [Gcap][M] per-group weights while wgroups > 0
+    int wgroups = 0;
     int k3_blocks = 0;
     // reprojection lines, keyed by the .tlt angle
     std::map<float, std::unique_ptr<NodeTables>> lines;
@@ -230,7 +232,12 @@ struct icon_plan {
         Geo g;
         g.N0 = N0; g.N1 = N1; g.n0 = n0; g.n1 = n1; g.lg0 = lg0; g.lg1 = lg1;
         g.M = t.M; g.nx = nx; g.nz = nz; g.B = B;
-        g.w = t.w; g.phix = t.phix; g.phiy = t.phiy; g.ix0 = t.ix0; g.iy0 = t.iy0;
+        g.w = t.w; g.wstride = 0;
+        if (&t == &nodes && wgroups > 0) {   // icon_plan_set_group_weights
+            g.w = wgroup;
+            g.wstride = (size_t)M;
+        }
+        g.phix = t.phix; g.phiy = t.phiy; g.ix0 = t.ix0; g.iy0 = t.iy0;
         g.cx = cx; g.cy = cy; g.rcx = rcx; g.rcy = rcy; g.row_off = t.row_off; g.ent_jt = t.ent_jt; g.ent_iy0 = t.ent_iy0;
         g.ent_lb = t.ent_lb; g.ent_phiy = t.ent_phiy; g.ent_pxy = t.ent_pxy;
         g.tw0 = tw0; g.tw1 = tw1;
@@ -715,6 +722,34 @@ icon_status icon_plan_geometry(const icon_plan *p, float *h_xy, float *h_w)
     if (!p) return fail(ICON_ERR_INVALID, "null plan");
     if (h_xy) std::memcpy(h_xy, p->xy.data(), sizeof(float) * p->xy.size());
     if (h_w) std::memcpy(h_w, p->w.data(), sizeof(float) * p->w.size());
+    return ICON_OK;
+}
+
+icon_status icon_weights(int nx, int ntilt, const float *tilt_deg, float *h_w)
+{
+    if (!tilt_deg || !h_w || nx < 2 || ntilt < 2) return fail(ICON_ERR_INVALID, "icon_weights: bad argument");
+    std::vector<float> neg(ntilt);
+    for (int i = 0; i < ntilt; ++i) neg[i] = -tilt_deg[i];   // the plan's node angles (MainCode.cu:46-49)
+    weights(nx, ntilt, neg.data(), h_w);
+    return ICON_OK;
+}
+
+icon_status icon_plan_set_group_weights(icon_plan *p, const float *h_w, int ngroups)
+{
+    if (!p) return fail(ICON_ERR_INVALID, "null plan");
+    if (ngroups == 0) {
+        p->wgroups = 0;
+        return ICON_OK;
+    }
+    if (!h_w || ngroups < 0 || ngroups > p->Gcap)
+        return fail(ICON_ERR_INVALID, "ngroups must be in 0.." + std::to_string(p->Gcap) + " with weights given");
+    DeviceGuard guard(p->dev);
+    const size_t M = (size_t)p->M;
+    if (!p->wgroup) ICON_TRY(p->arena.alloc(&p->wgroup, (size_t)p->Gcap * M));
+    ICON_CUDA(cudaMemcpy(p->wgroup, h_w, sizeof(float) * ngroups * M, cudaMemcpyHostToDevice));
+    for (int gi = ngroups; gi < p->Gcap; ++gi)   // the remaining groups keep the plan's own weights
+        ICON_CUDA(cudaMemcpy(p->wgroup + gi * M, p->nodes.w, sizeof(float) * M, cudaMemcpyDeviceToDevice));
+    p->wgroups = ngroups;
     return ICON_OK;
 }
 

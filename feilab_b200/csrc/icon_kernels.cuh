@@ -40,7 +40,8 @@ constexpr int kLdPhiy = 16;   // phiy rows padded to 16 floats (four 16-byte loa
 // Device view of one tilt-series geometry (all pointers are device memory).
 struct Geo {
     int N0, N1, n0, n1, lg0, lg1, M, nx, nz, B;
-    const float *w;        // [M] density weights (Weight, weight.cu:8-41)
+    const float *w;        // [M] density weights (Weight, weight.cu:8-41), group g's at w + g*wstride
+    size_t wstride;        // 0: one weight vector for every group; M: one per group
     const float *phix;     // [M][14] window values, x taps   (NU:221-235)
     const float *phiy;     // [M][16] window values, y taps, 2 zero pads
     const int *ix0;        // [M] first x tap, unwrapped: floor(n0*x0) - 6
@@ -394,10 +395,10 @@ __global__ void k_interp_fin(Geo g, const float2 *__restrict__ P, float2 *__rest
         if (MODE == 0) {
             f[((size_t)grp * g.M + j) * B + b] = acc;
         } else if (MODE == 1) {
-            float w = __ldg(&g.w[j]);
+            float w = __ldg(&g.w[(size_t)grp * g.wstride + j]);
             f[((size_t)grp * g.M + j) * B + b] = make_float2(acc.x * w, acc.y * w);
         } else {
-            double w = (double)__ldg(&g.w[j]);
+            double w = (double)__ldg(&g.w[(size_t)grp * g.wstride + j]);
             acc2 = (double)acc.x * (double)acc.x * w + (double)acc.y * (double)acc.y * w;
         }
     }
@@ -725,7 +726,7 @@ __global__ void FFT_BOUNDS(E) k_rows_fwd(Geo g, Geo1 g1, const float *__restrict
         int j = i * N + k;
         size_t o = ((size_t)grp * g.M + j) * B + b;
         if (bout) bout[o] = acc;
-        float w = __ldg(&g.w[j]);
+        float w = __ldg(&g.w[(size_t)grp * g.wstride + j]);
         f[o] = make_float2(acc.x * w, acc.y * w);
     }
 }

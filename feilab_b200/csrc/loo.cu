@@ -6,8 +6,17 @@
 // remaining tilts, readSlicePart_crossV.cu:3-34), reprojects at the omitted
 // angle (reProject_NFFT2, reProject_NFFT.cu:25-42) and compares with the
 // omitted projection by FRC (calFRC_nonsqure + frcSmooth).  Here every tilt
-// takes that role in turn: one plan per omitted tilt, the slices in batches
-// of the plan's capacity, FRC per omitted tilt.  Optionally each solve ends
+// takes that role in turn, and all the left-out solves run as one batched
+// schedule on one plan over all tilts: a work item is (omitted tilt k, B
+// consecutive slices), one slice group; a batch is as many items as the
+// capacity holds, each group with its own weights (icon_plan_set_group_weights):
+// tilt k's nodes at 0 and the other tilts weighted as Weight() weights the
+// series without k.  Weight 0 removes a node from every sum of the data
+// term, so a group solves exactly the reduced series (up to the order in
+// which the step length's double partial sums are combined), with no plan
+// rebuilt per tilt and full batches however few slices there are.  Each
+// group is reprojected at its omitted angle, and the FRC per omitted tilt
+// compares those with the omitted projection.  Optionally each batch ends
 // its ICON phase at a relative-step tolerance (icon_solve_until).  Every
 // solve starts from m = 0: a start that holds the omitted projection (such
 // as the reconstruction from all tilts) would leak it into the validation,
@@ -52,8 +61,30 @@ extern "C" icon_status icon_loo_sweep(const float *h_rows, int nx, int thickness
     if (!h_rows || !tilt_deg || !cfg || !h_frc || nx < 2 || thickness < 1 || nz < 3 || S < 1 || capacity < 1)
         return loo_fail(ICON_ERR_INVALID, "icon_loo_sweep: bad argument");
     if (cudaSetDevice(device) != cudaSuccess) return loo_fail(ICON_ERR_CUDA, "icon_loo_sweep: cudaSetDevice");
-    const int cap = std::min(capacity, S);
+    icon_status rc = ICON_OK;
+    // One plan over all tilts; its capacity bounds a batch.
+    const int cap = capacity;
+    icon_geometry g{nx, thickness, nz, tilt_deg, cap, device};
+    Plan P;
+    if ((rc = icon_plan_create(&g, &P.p)) != ICON_OK) return rc;
+    int dims[10];
+    if ((rc = icon_plan_query(P.p, dims)) != ICON_OK) return rc;
+    const int M = dims[4], B = dims[6];
+    const int per_item = std::min(B, cap);             // slices of one work item (one group)
+    const int items_per_batch = std::max(1, cap / B);  // groups of a batch
     const size_t NN = (size_t)nx * thickness;
+    // Weights of each left-out series, in the full plan's node order.
+    std::vector<float> wk((size_t)nz * M), wred((size_t)(nz - 1) * nx), t1(nz - 1);
+    for (int k = 0; k < nz; ++k) {
+        for (int i = 0, q = 0; i < nz; ++i)
+            if (i != k) t1[q++] = tilt_deg[i];
+        if ((rc = icon_weights(nx, nz - 1, t1.data(), wred.data())) != ICON_OK) return rc;
+        float *w = &wk[(size_t)k * M];
+        for (int i = 0, q = 0; i < nz; ++i) {
+            if (i == k) std::fill(w + (size_t)i * nx, w + (size_t)(i + 1) * nx, 0.f);
+            else std::memcpy(w + (size_t)i * nx, &wred[(size_t)q++ * nx], sizeof(float) * nx);
+        }
+    }
     cudaStream_t st = nullptr;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
         return loo_fail(ICON_ERR_CUDA, "icon_loo_sweep: stream");
@@ -61,46 +92,62 @@ extern "C" icon_status icon_loo_sweep(const float *h_rows, int nx, int thickness
         cudaStream_t s;
         ~StreamGuard() { cudaStreamDestroy(s); }
     } sg{st};
+    const int slots = items_per_batch * B > cap ? per_item : items_per_batch * B;
     DevArr rows, Ahwb, m, rp;
-    if (cudaMalloc(&rows.p, sizeof(float) * (size_t)cap * nz * nx) != cudaSuccess ||
-        cudaMalloc(&Ahwb.p, sizeof(float) * 2 * (size_t)cap * NN) != cudaSuccess ||
-        cudaMalloc(&m.p, sizeof(float) * (size_t)cap * NN) != cudaSuccess ||
-        cudaMalloc(&rp.p, sizeof(float) * (size_t)cap * nx) != cudaSuccess) {
+    if (cudaMalloc(&rows.p, sizeof(float) * (size_t)slots * nz * nx) != cudaSuccess ||
+        cudaMalloc(&Ahwb.p, sizeof(float) * 2 * (size_t)slots * NN) != cudaSuccess ||
+        cudaMalloc(&m.p, sizeof(float) * (size_t)slots * NN) != cudaSuccess ||
+        cudaMalloc(&rp.p, sizeof(float) * (size_t)slots * nx) != cudaSuccess) {
         cudaGetLastError();
         return loo_fail(ICON_ERR_NOMEM, "icon_loo_sweep: device memory");
     }
-    icon_status rc = ICON_OK;
-    std::vector<float> t1(nz - 1), r1((size_t)cap * (nz - 1) * nx), gt((size_t)S * nx), rps((size_t)S * nx);
-    for (int omit = 0; omit < nz; ++omit) {
-        for (int k = 0, q = 0; k < nz; ++k)
-            if (k != omit) t1[q++] = tilt_deg[k];
-        icon_geometry g{nx, thickness, nz - 1, t1.data(), cap, device};
-        Plan P;
-        if ((rc = icon_plan_create(&g, &P.p)) != ICON_OK) return rc;
-        int iters_max = 0;
-        for (int s0 = 0; s0 < S; s0 += cap) {
-            const int nb = std::min(cap, S - s0);
-            // rows of the batch without the omitted tilt (readSlicePart_crossV.cu:13-22)
-            for (int s = 0; s < nb; ++s)
-                for (int k = 0, q = 0; k < nz; ++k) {
-                    const float *src = h_rows + ((size_t)(s0 + s) * nz + k) * nx;
-                    if (k == omit) std::memcpy(&gt[(size_t)(s0 + s) * nx], src, sizeof(float) * nx);
-                    else std::memcpy(&r1[((size_t)s * (nz - 1) + q++) * nx], src, sizeof(float) * nx);
-                }
-            cudaMemcpyAsync(rows.p, r1.data(), sizeof(float) * (size_t)nb * (nz - 1) * nx, cudaMemcpyHostToDevice, st);
-            if ((rc = icon_prepare_rhs(P.p, (const float *)rows.p, Ahwb.p, nb, st)) != ICON_OK) return rc;
-            int it = 0;
-            rc = icon_solve_until(P.p, cfg, Ahwb.p, (float *)m.p, nb, 0, tol, 10, &it, nullptr, st);
-            if (rc != ICON_OK) return rc;
-            iters_max = std::max(iters_max, it);
-            if ((rc = icon_reproject(P.p, (const float *)m.p, tilt_deg[omit], (float *)rp.p, nb, st)) != ICON_OK) return rc;
-            cudaMemcpyAsync(&rps[(size_t)s0 * nx], rp.p, sizeof(float) * (size_t)nb * nx, cudaMemcpyDeviceToHost, st);
-            if (cudaStreamSynchronize(st) != cudaSuccess) return loo_fail(ICON_ERR_CUDA, "icon_loo_sweep: stream error");
+    // Work items in tilt-major order.
+    struct Item {
+        int k, s0, n;
+    };
+    std::vector<Item> items;
+    for (int k = 0; k < nz; ++k)
+        for (int s0 = 0; s0 < S; s0 += per_item) items.push_back({k, s0, std::min(per_item, S - s0)});
+    std::vector<float> hrows((size_t)slots * nz * nx), hw((size_t)items_per_batch * M), hrp((size_t)slots * nx);
+    std::vector<float> rps((size_t)nz * S * nx);
+    std::vector<int> iters(nz, 0);
+    for (size_t i0 = 0; i0 < items.size(); i0 += items_per_batch) {
+        const int ni = (int)std::min<size_t>(items_per_batch, items.size() - i0);
+        const int Sb = (ni - 1) * B + items[i0 + ni - 1].n;   // slots up to the last item's last slice
+        std::fill(hrows.begin(), hrows.end(), 0.f);          // padding slots solve zero data
+        for (int q = 0; q < ni; ++q) {
+            const Item &it = items[i0 + q];
+            std::memcpy(&hrows[(size_t)q * B * nz * nx], h_rows + (size_t)it.s0 * nz * nx, sizeof(float) * (size_t)it.n * nz * nx);
+            std::memcpy(&hw[(size_t)q * M], &wk[(size_t)it.k * M], sizeof(float) * M);
         }
-        if (h_reproj) std::memcpy(h_reproj + (size_t)omit * S * nx, rps.data(), sizeof(float) * (size_t)S * nx);
-        if (h_iters) h_iters[omit] = iters_max;
-        // FRC of the reprojection against the omitted projection (ICONGPU.cu:560-586)
-        if ((rc = icon_frc(gt.data(), rps.data(), nx, S, 10, h_frc + (size_t)omit * (nx / 2))) != ICON_OK) return rc;
+        if ((rc = icon_plan_set_group_weights(P.p, hw.data(), ni)) != ICON_OK) return rc;
+        cudaMemcpyAsync(rows.p, hrows.data(), sizeof(float) * (size_t)Sb * nz * nx, cudaMemcpyHostToDevice, st);
+        if ((rc = icon_prepare_rhs(P.p, (const float *)rows.p, Ahwb.p, Sb, st)) != ICON_OK) return rc;
+        int done = 0;
+        if ((rc = icon_solve_until(P.p, cfg, Ahwb.p, (float *)m.p, Sb, 0, tol, 10, &done, nullptr, st)) != ICON_OK) return rc;
+        for (int q = 0; q < ni; ++q) {
+            const Item &it = items[i0 + q];
+            iters[it.k] = std::max(iters[it.k], done);
+            if ((rc = icon_reproject(P.p, (const float *)m.p + (size_t)q * B * NN, tilt_deg[it.k],
+                                     (float *)rp.p + (size_t)q * B * nx, it.n, st)) != ICON_OK)
+                return rc;
+        }
+        cudaMemcpyAsync(hrp.data(), rp.p, sizeof(float) * (size_t)Sb * nx, cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) return loo_fail(ICON_ERR_CUDA, "icon_loo_sweep: stream error");
+        for (int q = 0; q < ni; ++q) {
+            const Item &it = items[i0 + q];
+            std::memcpy(&rps[((size_t)it.k * S + it.s0) * nx], &hrp[(size_t)q * B * nx], sizeof(float) * (size_t)it.n * nx);
+        }
     }
+    // FRC of each omitted tilt's reprojections against its projection (ICONGPU.cu:560-586).
+    std::vector<float> gt((size_t)S * nx);
+    for (int k = 0; k < nz; ++k) {
+        for (int s = 0; s < S; ++s)
+            std::memcpy(&gt[(size_t)s * nx], h_rows + ((size_t)s * nz + k) * nx, sizeof(float) * nx);
+        if ((rc = icon_frc(gt.data(), &rps[(size_t)k * S * nx], nx, S, 10, h_frc + (size_t)k * (nx / 2))) != ICON_OK)
+            return rc;
+        if (h_iters) h_iters[k] = iters[k];
+    }
+    if (h_reproj) std::memcpy(h_reproj, rps.data(), sizeof(float) * rps.size());
     return ICON_OK;
 }

@@ -54,6 +54,8 @@ def lib():
         L.icon_host_free.argtypes = [V]
         L.icon_stack_upload.argtypes = [I, V, I, I, I, I, I, ctypes.POINTER(V), V]
         L.icon_device_free.argtypes = [I, V]
+        L.icon_weights.argtypes = [I, I, V, V]
+        L.icon_plan_set_group_weights.argtypes = [P, V, I]
         L.icon_trace_enable.argtypes = [P, I]
         L.icon_trace_read.argtypes = [P, V, V, V]
         L.icon_launch_count.argtypes = [P]
@@ -64,7 +66,7 @@ def lib():
                      "icon_rows_forward", "icon_prepare_rhs", "icon_solve", "icon_solve_until", "icon_reproject",
                      "icon_reconstruct_host", "icon_trace_enable", "icon_trace_read", "icon_prepare_rhs_stack",
                      "icon_reconstruct_stack", "icon_reconstruct_stack_host", "icon_host_alloc", "icon_host_free",
-                     "icon_stack_upload", "icon_device_free"):
+                     "icon_stack_upload", "icon_device_free", "icon_weights", "icon_plan_set_group_weights"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -130,6 +132,16 @@ class IconPlan:
             self._h = None
 
     __del__ = close
+
+    def set_group_weights(self, w=None):
+        """Per-group density weights (ngroups, M) float32 for slice groups
+        0..ngroups-1 of later calls (B slices each); None restores the
+        plan's own weights."""
+        if w is None:
+            _check(lib().icon_plan_set_group_weights(self._h, None, 0))
+            return
+        w = np.ascontiguousarray(np.asarray(w, np.float32).reshape(-1, self.M))
+        _check(lib().icon_plan_set_group_weights(self._h, w.ctypes.data_as(ctypes.c_void_p), w.shape[0]))
 
     def geometry(self):
         xy = np.zeros((self.M, 2), np.float32)
@@ -365,3 +377,12 @@ def host_alloc(nbytes):
     p = ctypes.c_void_p()
     _check(lib().icon_host_alloc(int(nbytes), ctypes.byref(p)))
     return p.value, lambda: lib().icon_host_free(ctypes.c_void_p(p.value))
+
+
+def weights(nx, tilts):
+    """Density weights (ntilt, nx) of a tilt series given as in the .tlt
+    file, as the plan weights its nodes (icon_weights; Weight, weight.cu:8-41)."""
+    t = np.ascontiguousarray(np.asarray(tilts, np.float32))
+    w = np.zeros((len(t), int(nx)), np.float32)
+    _check(lib().icon_weights(int(nx), len(t), t.ctypes.data_as(ctypes.c_void_p), w.ctypes.data_as(ctypes.c_void_p)))
+    return w

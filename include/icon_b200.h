@@ -98,6 +98,23 @@ icon_status icon_plan_query(const icon_plan *plan, int *dims);
  * Either pointer may be NULL. */
 icon_status icon_plan_geometry(const icon_plan *plan, float *h_xy, float *h_w);
 
+/* h_w[ntilt*nx] <- the density weights of a tilt series given as in the
+ * .tlt file, as Weight() computes them for the plan's nodes
+ * (weight.cu:8-41); tilt i's nodes are h_w[i*nx .. i*nx+nx-1]. */
+icon_status icon_weights(int nx, int ntilt, const float *tilt_deg, float *h_w);
+
+/* Per-group density weights: slice group g of every later call (slices
+ * g*B .. g*B+B-1, B = icon_plan_query dims[6]) uses h_w[g][M] in place of
+ * the plan's own weights, for g < ngroups (<= capacity / B rounded up); the
+ * other groups keep the plan's.  ngroups = 0 restores the plan's weights
+ * for all.  A node of weight 0 drops out of the data term: with one tilt's
+ * nodes at 0 and the others weighted as icon_weights gives for the series
+ * without it, a group solves that series (the left-out solves of
+ * icon_loo_sweep, all tilts in one batched schedule).  Copies h_w to the
+ * device (synchronous).  No counterpart in the reference, whose plans hold
+ * one weight vector. */
+icon_status icon_plan_set_group_weights(icon_plan *plan, const float *h_w, int ngroups);
+
 /* Forward 2-D NUFFT of real images: d_nodes = A d_img.
  * Replaces cunfft_trafo_2d_R2C2 (NU:984-1076). */
 icon_status icon_nufft_forward(icon_plan *plan, const float *d_img, void *d_nodes, int S, void *stream);

@@ -84,9 +84,13 @@ icon_status icon_frc(const float *a, const float *b, int nx, int ny, int smooth_
  * reconstructs without it, reprojects at its angle and compares with the
  * omitted projection by FRC.  This call does that for each of the nz tilts
  * in turn: h_rows [S][nz][nx] (host; rows of every tilt per slice),
- * thickness, tilt_deg[nz], the solve schedule cfg; plans of `capacity`
- * slices on `device`.  tol > 0 ends each ICON phase at that relative step
- * (icon_solve_until); tol = 0 is the reference's solve for every tilt.
+ * thickness, tilt_deg[nz], the solve schedule cfg, on `device`.  All nz*S
+ * left-out solves run as one batched schedule on one plan over all tilts of
+ * `capacity` slots: each slice group is (omitted tilt, B slices) with that
+ * tilt's nodes weighted 0 and the rest weighted for the series without it
+ * (icon_plan_set_group_weights), which solves the reduced series.  tol > 0
+ * ends each batch's ICON phase at that relative step (icon_solve_until);
+ * tol = 0 is the reference's solve for every tilt.
  * Solves start from m = 0: a start holding the omitted projection (the
  * reconstruction from all tilts, say) would leak it into the validation.
  * h_frc [nz][nx/2] receives the

@@ -59,3 +59,58 @@ def test_loo_with_tolerance_stops_within_schedule(golden):
     a, b, c = [int(v) for v in z["sched"]]
     assert np.all(it_t <= it_c) and np.all(it_t >= a + c)
     assert np.all(np.isfinite(frc_t))
+
+
+def _reduced_plan_reprojection(z, omit):
+    """The left-out solve of one tilt with a plan built for the series
+    without it (the reference's own construction)."""
+    import torch
+    from feilab_b200.icon import IconPlan
+    keep = [k for k in range(len(z["tilts"])) if k != omit]
+    S = int(z["S"])
+    p = IconPlan(int(z["nx"]), int(z["thickness"]), z["tilts"][keep], capacity=S)
+    rows = torch.from_numpy(np.ascontiguousarray(z["rows"][:, keep])).cuda()
+    m = p.solve(p.prepare_rhs(rows), tuple(int(v) for v in z["sched"]), int(z["data_type"]), float(z["threshold"]))
+    return p.reproject(m, float(z["tilts"][omit])).cpu().numpy()
+
+
+@pytest.mark.parametrize("capacity", [4, 24])
+def test_batched_sweep_equals_per_tilt_plans(golden, capacity):
+    # One plan over all tilts with per-group weights (omitted tilt at 0)
+    # against a plan built without the tilt: the same solve, up to the order
+    # in which the step length's double partial sums are combined.
+    z = golden["cli"]
+    frc, rp, _ = _sweep(z) if capacity == 4 else _sweep_cap(z, capacity)
+    nz = len(z["tilts"])
+    for omit in (0, nz // 2, nz - 1):
+        ref = _reduced_plan_reprojection(z, omit)
+        assert rel_l2(rp[omit], ref) < 1e-6, omit
+
+
+def _sweep_cap(z, capacity):
+    from feilab_b200 import tools
+    return tools.loo_sweep(z["rows"], int(z["thickness"]), z["tilts"], tuple(int(v) for v in z["sched"]),
+                           int(z["data_type"]), float(z["threshold"]), capacity=capacity)
+
+
+def test_group_weights_set_and_restore(golden):
+    import torch
+    from feilab_b200.icon import IconPlan, weights
+    z = golden["a"]
+    S = int(z["S"])
+    p = IconPlan(int(z["nx"]), int(z["thickness"]), z["tilts"], capacity=S)
+    rows = torch.from_numpy(np.ascontiguousarray(z["rows"])).cuda()
+    sched = tuple(int(v) for v in z["sched"])
+    plain = p.solve(p.prepare_rhs(rows), sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+    # the plan's own weights given per group change nothing
+    w = weights(int(z["nx"]), z["tilts"]).ravel()
+    p.set_group_weights(np.stack([w] * ((S + p.B - 1) // p.B)))
+    same = p.solve(p.prepare_rhs(rows), sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+    assert np.array_equal(same, plain)
+    # zero weights remove the data term: the solve stays at m = 0
+    p.set_group_weights(np.zeros((1, p.M), np.float32))
+    zero = p.solve(p.prepare_rhs(rows), sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+    assert not np.any(zero[:min(S, p.B)]) and np.array_equal(zero[p.B:], plain[p.B:])
+    p.set_group_weights(None)
+    back = p.solve(p.prepare_rhs(rows), sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+    assert np.array_equal(back, plain)

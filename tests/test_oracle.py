@@ -172,3 +172,14 @@ def test_frc_matches_reference_crossv_file(golden, tmp_path):
     got = tools.frc(imgs[0], imgs[1], 10)
     assert got.shape == (ref.shape[0],)
     np.testing.assert_allclose(got, ref[:, 1], atol=2e-6)
+
+
+def test_icon_weights_match_oracle_weights():
+    # icon_weights (the weights a plan gives its nodes, also used for the
+    # left-out series of icon_loo_sweep) against the oracle's Weight().
+    from feilab_b200.icon import weights
+    for nx, tilts in [(64, np.linspace(-60, 60, 31)), (50, np.array([-47.0, -20.5, 3.0, 8.0, 52.0])),
+                      (128, np.delete(np.arange(-60, 61, 2.0), [0, 30]))]:
+        t = np.asarray(tilts, np.float32)
+        _, w_o, _ = OraclePlan(nx, 16, t, "f64").geometry()
+        assert np.array_equal(weights(nx, t).ravel(), w_o)
