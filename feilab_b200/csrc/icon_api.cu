@@ -364,6 +364,11 @@ icon_status build_tables(icon_plan *p, const float *xy, const float *w, int M, N
         }
         if (c > a && (ky2[a] + r0ofs < 0 || ky2[c - 1] + r0ofs + kTaps > p->n1 + 2 * icon::kHalo))
             return fail(ICON_ERR_INVALID, "window taps outside the rotated y buffer");
+        // The mirrored windows of the real-image forward y-pass: buffer rows
+        // n1/2 - iy0 + kHalo - 13 .. n1/2 - iy0 + kHalo.
+        if (c > a && (p->n1 / 2 - ky2[c - 1] + icon::kHalo - (kTaps - 1) < 0 ||
+                      p->n1 / 2 - ky2[a] + icon::kHalo > p->n1 + 2 * icon::kHalo - 1))
+            return fail(ICON_ERR_INVALID, "mirrored window taps outside the rotated y buffer");
     }
     ICON_TRY(p->arena.upload(&t.row_off, cnt.data(), (size_t)n0 + 1));
     ICON_TRY(p->arena.upload(&t.ent_jt, jt2.data(), E));
@@ -397,15 +402,17 @@ inline int grid1d(size_t total)
 // Algorithmic bytes per slot (one slice of a group) of each stage: the data a
 // stage must read and write at least once; per-group tables are divided by B.
 struct StageBytes {
-    double xf_real, xf_cplx, yf, fin_store, fin_red, ya, xa_plain, xa_resid, upd;
+    double xf_real, xf_cplx, yf, yf_real, fin_store, fin_red, ya, xa_plain, xa_resid, upd;
 };
 StageBytes stage_bytes(const icon_plan *p, const NodeTables &t)
 {
     StageBytes b;
     double NN = (double)p->N0 * p->N1, G1 = (double)p->n0 * p->N1 * 8, MT = (double)t.M * kTaps, B = p->B;
-    b.xf_real = NN * 4 + G1;
+    const double G1h = (double)(p->n0 / 2 + 1) * p->N1 * 8;   // rows 0..n0/2 (real image)
+    b.xf_real = NN * 4 + G1h;
     b.xf_cplx = NN * 8 + G1;
     b.yf = G1 + MT * 8 + (MT * 8 + MT * 4) / B;            // G1 row reads, P writes; entries + phiy
+    b.yf_real = G1h + MT * 8 + (MT * 8 + MT * 4) / B;
     b.fin_store = MT * 8 + (double)t.M * 8 + (MT * 4 + t.M * 4) / B;
     b.fin_red = MT * 8 + (MT * 4 + t.M * 4) / B;
     b.ya = (double)t.M * 8 + G1 + (MT * 8 + MT * 8) / B;   // f, G1 writes; entries + phix/phiy
@@ -421,11 +428,14 @@ icon_status launch_forward(icon_plan *p, const NodeTables &t, const void *img_in
     Geo g = p->geo(t);
     const StageBytes sb = stage_bytes(p, t);
     const double slots = (double)G * p->B;
-    dim3 gx(p->N1, G), gy(G, p->n0);
+    // A real image's spectrum is Hermitian: the y-pass takes grid rows
+    // 0..n0/2 and interpolates the mirror rows' entries from them.
+    dim3 gx(p->N1, G), gy(G, real_in ? p->n0 / 2 + 1 : p->n0);
     WITH_B(p->B,
         LAUNCH_B(p, K_XF, st, (real_in ? sb.xf_real : sb.xf_cplx) * slots,
                  L::xpass_fwd(real_in, p->ex, gx, p->thr_x, p->smem_x, st, g, img_int, p->G1));
-        LAUNCH_B(p, K_YF, st, sb.yf * slots, L::ypass_fwd(p->ey, gy, p->thr_y, p->smem_y, st, g, p->G1, p->P)))
+        LAUNCH_B(p, K_YF, st, (real_in ? sb.yf_real : sb.yf) * slots,
+                 L::ypass_fwd(p->ey, real_in, gy, p->thr_y, p->smem_y, st, g, p->G1, p->P)))
     int kb = (t.M * p->B + 255) / 256;
     dim3 g3(kb, G);
     WITH_B(p->B,

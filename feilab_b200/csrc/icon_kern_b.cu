@@ -24,11 +24,16 @@ void Launch<B>::xpass_fwd(bool real_in, int E, dim3 grid, int threads, size_t sm
 }
 
 template <int B>
-void Launch<B>::ypass_fwd(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const float2 *G1,
-                          float2 *P)
+void Launch<B>::ypass_fwd(int E, bool herm, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
+                          const float2 *G1, float2 *P)
 {
-    if (E == 32) k_ypass_fwd<B, 32><<<grid, threads, smem, st>>>(g, G1, P);
-    else k_ypass_fwd<B, 16><<<grid, threads, smem, st>>>(g, G1, P);
+    if (E == 32) {
+        if (herm) k_ypass_fwd<B, 32, true><<<grid, threads, smem, st>>>(g, G1, P);
+        else k_ypass_fwd<B, 32, false><<<grid, threads, smem, st>>>(g, G1, P);
+    } else {
+        if (herm) k_ypass_fwd<B, 16, true><<<grid, threads, smem, st>>>(g, G1, P);
+        else k_ypass_fwd<B, 16, false><<<grid, threads, smem, st>>>(g, G1, P);
+    }
 }
 
 template <int B>
@@ -119,10 +124,12 @@ cudaError_t Launch<B>::set_smem(int ex, int ey, size_t smem_x, size_t need_x, si
         set((const void *)k_row_adj<B, 16>, smem_x);
     }
     if (ey == 32) {
-        set((const void *)k_ypass_fwd<B, 32>, smem_y);
+        set((const void *)k_ypass_fwd<B, 32, false>, smem_y);
+        set((const void *)k_ypass_fwd<B, 32, true>, smem_y);
         set((const void *)k_ypass_adj<B, 32, false>, smem_ya);
     } else {
-        set((const void *)k_ypass_fwd<B, 16>, smem_y);
+        set((const void *)k_ypass_fwd<B, 16, false>, smem_y);
+        set((const void *)k_ypass_fwd<B, 16, true>, smem_y);
         set((const void *)k_ypass_adj<B, 16, false>, smem_ya);
         set((const void *)k_ypass_adj<B, 16, true>, smem_ya);
     }

@@ -178,7 +178,11 @@ __global__ void FFT_BOUNDS(E) k_xpass_fwd(Geo g, const void *__restrict__ in, fl
         float2 v = reinterpret_cast<const float2 *>(raw)[X * B + b];
         return make_float2(v.x * r, v.y * r);
     };
-    auto st = [=](int x, int b, float2 v) { out[(size_t)x * N1 * B + b] = v; };
+    // A real image's rows n0/2+1.. are the conjugates of rows n0/2-1..1;
+    // the forward y-pass (HERM) reads rows 0..n0/2 only.
+    auto st = [=](int x, int b, float2 v) {
+        if (!REAL_IN || x <= (n >> 1)) out[(size_t)x * N1 * B + b] = v;
+    };
     fft_fused<B, B, E>(s, n, g.lg0, g.tw0, -1.f, ld, st);
 }
 
@@ -230,13 +234,22 @@ __host__ __device__ inline size_t ypass_fwd_smem(int n1, int B)
 // entries are copied behind it; the FFT waits only for the row.  One thread
 // per entry then computes all B slices of it from the rotated row; entries
 // past the copied ones are loaded one round ahead.
-template <int B, int E>
+//
+// HERM (the forward transform of a real image, cunfft_trafo_2d_R2C2,
+// NU:984-1076, whose cuFFT R2C keeps half the spectrum): G1 row n0 - x is the
+// conjugate of row x, so its FFT along y is the conjugate mirror of row x's,
+// buf'[q] = conj(buf[-q mod n1]).  The grid then covers rows x = 0..n0/2
+// only; each CTA also interpolates the entries of row n0 - x, reading the 14
+// taps of an entry from the mirrored window in reverse order and storing the
+// conjugate of the sum.  The x-pass writes only rows 0..n0/2 of G1.
+template <int B, int E, bool HERM>
 __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, float2 *__restrict__ P)
 {
     extern __shared__ float2 s[];
     constexpr int SB = YfStride<B>::v;
     constexpr bool kPairs = (B == 8);   // 64-byte rows read as 128-byte row pairs
     const int grp = blockIdx.x, x = blockIdx.y, n = g.n1, N1 = g.N1;
+    const int xp = (g.n0 - x) & (g.n0 - 1);   // the mirror row (HERM)
     const int T = blockDim.x;
     const float2 *rowin = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
     float2 *row = s + kHalo * SB;
@@ -245,7 +258,13 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
     int *pre_iy = pre_jt + kPreEntries;                                                 // [kPreEntries]
     float2 *tw_s = reinterpret_cast<float2 *>(pre_iy + kPreEntries);                    // [n] twiddles
     const float2 *tws = ypass_tw_shared(n) ? tw_s : g.tw1;
-    const int e0 = g.row_off[x], cnt = g.row_off[x + 1] - e0;
+    // Entries: row x's (ca of them), then with HERM and xp != x the mirror
+    // row's (cb); i-th entry of the combined list at global index ent(i).
+    const int ea = g.row_off[x], ca = g.row_off[x + 1] - ea;
+    const int eb = (HERM && xp != x) ? g.row_off[xp] : 0;
+    const int cb = (HERM && xp != x) ? g.row_off[xp + 1] - eb : 0;
+    const int cnt = ca + cb;
+    auto ent = [=](int i) { return i < ca ? ea + i : eb + (i - ca); };
     const int staged = min(cnt, min(T, kPreEntries));
     // Group 1: the N1 nonzero values of the row (contiguous in G1) and the
     // FFT's twiddle table.
@@ -254,7 +273,7 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
     cp_async_commit();
     // Group 2: tables of the first entries.
     if ((int)threadIdx.x < staged) {
-        const int e = e0 + threadIdx.x;
+        const int e = ent(threadIdx.x);
         const float *src = g.ent_phiy + (size_t)e * kLdPhiy;
         float *dst = pre_phi + threadIdx.x * kLdPhiy;
 #pragma unroll
@@ -298,21 +317,27 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
 #pragma unroll
         for (int q = 0; q < 4; ++q) cur.py[q] = py4[q];
     } else if (i < cnt) {
-        load_global(e0 + i, cur);
+        load_global(ent(i), cur);
     }
     while (i < cnt) {
         const int i2 = i + T;             // never among the copied entries (staged <= T)
-        if (i2 < cnt) load_global(e0 + i2, nxt);
+        if (i2 < cnt) load_global(ent(i2), nxt);
         const int j = cur.jt >> 4, t0 = cur.jt & 15;
-        const float2 *sr = s + (cur.iy + rofs) * SB;
-        float py[16];
+        // A mirror-row entry's tap t1 is buffer row rm - t1, rm = n1/2 - iy0
+        // + kHalo: the window starts at rm - 13 and is read in reverse.
+        const bool mir = HERM && i >= ca;
+        const int r0 = mir ? (n / 2 - cur.iy + kHalo - (kTaps - 1)) : (cur.iy + rofs);
+        const float2 *sr = s + r0 * SB;
+        float py0[16], py[kTaps];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            py[4 * q] = cur.py[q].x;
-            py[4 * q + 1] = cur.py[q].y;
-            py[4 * q + 2] = cur.py[q].z;
-            py[4 * q + 3] = cur.py[q].w;
+            py0[4 * q] = cur.py[q].x;
+            py0[4 * q + 1] = cur.py[q].y;
+            py0[4 * q + 2] = cur.py[q].z;
+            py0[4 * q + 3] = cur.py[q].w;
         }
+#pragma unroll
+        for (int t1 = 0; t1 < kTaps; ++t1) py[t1] = mir ? py0[kTaps - 1 - t1] : py0[t1];
         if constexpr (kPairs) {
             // Taps 2p and 2p+1 are rows r and r+1, one 128-byte block = eight
             // 16-byte chunks (chunk c: row r + c/4, slices 2(c%4), 2(c%4)+1),
@@ -322,7 +347,6 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
             // rows of the lanes' entries.  acc[k % 4] then always holds the
             // slices of quad (l + k) % 4.
             const int lane8 = threadIdx.x & 7;
-            const int r0 = cur.iy + rofs;
             const char *rb = reinterpret_cast<const char *>(s) + (size_t)r0 * (SB * sizeof(float2));
             const int o = lane8 + ((r0 & 1) << 2);
             float4 acc[4];
@@ -345,7 +369,10 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
             }
             float4 *dst = reinterpret_cast<float4 *>(P + pbase + ((size_t)j * kTaps + t0) * B);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) dst[(lane8 + k) & 3] = acc[k];
+            for (int k = 0; k < 4; ++k) {
+                if (mir) acc[k] = make_float4(acc[k].x, -acc[k].y, acc[k].z, -acc[k].w);
+                dst[(lane8 + k) & 3] = acc[k];
+            }
         } else {
             float2 acc[B];
 #pragma unroll
@@ -359,6 +386,10 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
                     acc[b].x = fmaf(v[b].x, py[t1], acc[b].x);
                     acc[b].y = fmaf(v[b].y, py[t1], acc[b].y);
                 }
+            }
+            if (mir) {
+#pragma unroll
+                for (int b = 0; b < B; ++b) acc[b].y = -acc[b].y;
             }
             store_b<B>(P + pbase + ((size_t)j * kTaps + t0) * B, acc);
         }

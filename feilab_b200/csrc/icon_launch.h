@@ -13,7 +13,7 @@ template <int B>
 struct Launch {
     static void xpass_fwd(bool real_in, int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
                           const void *in, float2 *G1);
-    static void ypass_fwd(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const float2 *G1,
+    static void ypass_fwd(int E, bool herm, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const float2 *G1,
                           float2 *P);
     static void interp_fin(int mode, dim3 grid, cudaStream_t st, const Geo &g, const float2 *P, float2 *f, double *part);
     static void ypass_adj(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const float2 *f,
