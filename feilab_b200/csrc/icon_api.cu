@@ -183,7 +183,7 @@ struct icon_plan {
     NodeTables nodes;
     float *cx = nullptr, *cy = nullptr, *rcx = nullptr, *rcy = nullptr, *phi1 = nullptr;
     int *i10 = nullptr;
-    float2 *tw0 = nullptr, *tw1 = nullptr;
+    float2 *tw0 = nullptr, *tw0h = nullptr, *tw1 = nullptr;
     // scratch sized for Gcap groups
     float2 *G1 = nullptr, *P = nullptr, *f = nullptr, *rhat = nullptr, *Ahwb = nullptr, *imgc = nullptr;
     float *m = nullptr, *rows = nullptr, *outrp = nullptr, *mout = nullptr;
@@ -240,7 +240,7 @@ struct icon_plan {
         g.phix = t.phix; g.phiy = t.phiy; g.ix0 = t.ix0; g.iy0 = t.iy0;
         g.cx = cx; g.cy = cy; g.rcx = rcx; g.rcy = rcy; g.row_off = t.row_off; g.ent_jt = t.ent_jt; g.ent_iy0 = t.ent_iy0;
         g.ent_lb = t.ent_lb; g.ent_phiy = t.ent_phiy; g.ent_pxy = t.ent_pxy;
-        g.tw0 = tw0; g.tw1 = tw1;
+        g.tw0 = tw0; g.tw0h = tw0h; g.tw1 = tw1;
         return g;
     }
     Geo1 geo1() const
@@ -640,8 +640,9 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
     ICON_TRY(p->arena.alloc(&p->i10, (size_t)nx));
     icon::k_window<<<(nx + 255) / 256, 256>>>(px1_d, 1, nx, p->n0, p->b0, p->bf0, p->phi1, kTaps, p->i10);
     ICON_CUDA(cudaGetLastError());
-    std::vector<float2> t0 = twiddles(p->n0), t1 = twiddles(p->n1);
+    std::vector<float2> t0 = twiddles(p->n0), t0h = twiddles(p->n0 / 2), t1 = twiddles(p->n1);
     ICON_TRY(p->arena.upload(&p->tw0, t0.data(), t0.size()));
+    ICON_TRY(p->arena.upload(&p->tw0h, t0h.data(), t0h.size()));
     ICON_TRY(p->arena.upload(&p->tw1, t1.data(), t1.size()));
     // Launch shapes: an FFT thread owns E values of an [n][B] batch: 32 when
     // radix-32 passes need fewer passes than radix-16 ones and the block still

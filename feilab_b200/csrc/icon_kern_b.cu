@@ -14,6 +14,11 @@ template <int B>
 void Launch<B>::xpass_fwd(bool real_in, int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
                           const void *in, float2 *G1)
 {
+    if (real_in && g.n0 / 2 >= E) {   // half-length FFT per slice: half the threads and buffer
+        if (E == 32) k_xpass_fwd_r2c<B, 32><<<grid, threads / 2, smem / 2, st>>>(g, (const float *)in, G1);
+        else k_xpass_fwd_r2c<B, 16><<<grid, threads / 2, smem / 2, st>>>(g, (const float *)in, G1);
+        return;
+    }
     if (E == 32) {
         if (real_in) k_xpass_fwd<true, B, 32><<<grid, threads, smem, st>>>(g, in, G1);
         else k_xpass_fwd<false, B, 32><<<grid, threads, smem, st>>>(g, in, G1);
@@ -111,6 +116,7 @@ cudaError_t Launch<B>::set_smem(int ex, int ey, size_t smem_x, size_t need_x, si
     if (ex == 32) {
         set((const void *)k_xpass_fwd<true, B, 32>, smem_x);
         set((const void *)k_xpass_fwd<false, B, 32>, smem_x);
+        set((const void *)k_xpass_fwd_r2c<B, 32>, smem_x / 2);
         set((const void *)k_xpass_adj<0, B, 32>, need_x);
         set((const void *)k_xpass_adj<1, B, 32>, need_x);
         set((const void *)k_rows_fwd<B, 32>, smem_x);
@@ -118,6 +124,7 @@ cudaError_t Launch<B>::set_smem(int ex, int ey, size_t smem_x, size_t need_x, si
     } else {
         set((const void *)k_xpass_fwd<true, B, 16>, smem_x);
         set((const void *)k_xpass_fwd<false, B, 16>, smem_x);
+        set((const void *)k_xpass_fwd_r2c<B, 16>, smem_x / 2);
         set((const void *)k_xpass_adj<0, B, 16>, need_x);
         set((const void *)k_xpass_adj<1, B, 16>, need_x);
         set((const void *)k_rows_fwd<B, 16>, smem_x);

@@ -57,6 +57,7 @@ struct Geo {
     const float *ent_phiy; // [M*14][16] phiy of the entry's node, in entry order
     const float *ent_pxy;  // [M*14][16] phix[j][t0] * phiy[j][t1], in entry order
     const float2 *tw0;     // [n0] exp(-2 pi i q / n0)
+    const float2 *tw0h;    // [n0/2] exp(-2 pi i q / (n0/2))
     const float2 *tw1;     // [n1] exp(-2 pi i q / n1)
 };
 
@@ -184,6 +185,50 @@ __global__ void FFT_BOUNDS(E) k_xpass_fwd(Geo g, const void *__restrict__ in, fl
         if (!REAL_IN || x <= (n >> 1)) out[(size_t)x * N1 * B + b] = v;
     };
     fft_fused<B, B, E>(s, n, g.lg0, g.tw0, -1.f, ld, st);
+}
+
+// Forward x-pass of a real image (the reference's R2C transform,
+// NU:984-1076) with half-length FFTs: the n0 real values x(t) of a slice's
+// column are packed as z(m) = x(2m) + i x(2m+1), m < N = n0/2, one FFT of
+// length N per slice (blockDim = N*B/E), and with Z = FFT(z), W = exp(-2 pi i/n0):
+//   X(k) = (Z(k) + conj Z(N-k)) / 2 - i W^k (Z(k) - conj Z(N-k)) / 2,
+// indices of Z mod N, written for k = 0..n0/2 (the rows the Hermitian y-pass
+// reads).  Each slice stays its own transform, so results do not depend on
+// which slices share a group.
+template <int B, int E>
+__global__ void FFT_BOUNDS(E) k_xpass_fwd_r2c(Geo g, const float *__restrict__ in, float2 *__restrict__ G1)
+{
+    extern __shared__ float2 s[];
+    const int Y = blockIdx.x, grp = blockIdx.y, n = g.n0, N = g.n0 / 2, N0 = g.N0, N1 = g.N1;
+    const float rcyY = g.rcy[Y];
+    const size_t ibase = ((size_t)grp * N1 + Y) * N0 * B;
+    float2 *out = G1 + (size_t)grp * n * N1 * B + (size_t)Y * B;
+    // The column [N0][B] and 1/cx, read by the first FFT pass before it
+    // writes s (N0 <= n0/2, so both fit in the N*B*8 bytes of s).
+    char *raw = reinterpret_cast<char *>(s);
+    float *rcs = reinterpret_cast<float *>(raw + (((size_t)N0 * B * sizeof(float) + 15) & ~(size_t)15));
+    copy_async(raw, in + ibase, (size_t)N0 * B * sizeof(float));
+    copy_async(rcs, g.rcx, (size_t)N0 * sizeof(float));
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    const float *rin = reinterpret_cast<const float *>(raw);
+    auto xval = [=](int t, int b) -> float {
+        int X = (t + N0 / 2) & (n - 1);
+        return X < N0 ? rin[X * B + b] * (rcs[X] * rcyY) : 0.f;
+    };
+    auto ld = [=](int m, int b) -> float2 { return make_float2(xval(2 * m, b), xval(2 * m + 1, b)); };
+    auto st = [=](int k, int b, float2 v) { s[k * B + b] = v; };
+    fft_fused<B, B, E>(s, N, g.lg0 - 1, g.tw0h, -1.f, ld, st);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < (N + 1) * B; idx += blockDim.x) {
+        const int k = idx / B, b = idx - k * B;
+        const float2 zk = s[(k & (N - 1)) * B + b], zm = s[((N - k) & (N - 1)) * B + b];
+        const float2 fe = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 fo = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+        const float2 w = __ldg(&g.tw0[k]);
+        out[(size_t)k * N1 * B + b] = cadd(fe, cmul(w, fo));
+    }
 }
 
 // Copies the wrap-around halo rows of a rotated row buffer (rows 0..7 and
