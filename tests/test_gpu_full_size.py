@@ -4,7 +4,9 @@ The golden fixtures are small (up to 256 wide); the kernels take other paths
 at production sizes: 8-slice groups with unpadded row pairs in the forward
 y-pass and two-row strips in the adjoint gather at 1024 x 300, 4-slice
 groups and an oversampled width of 4096 at 2048, short rows and odd widths
-elsewhere.  These cases run the operator on the shapes of the 1024x1024x300
+elsewhere, long y rows (thickness 700 and 1100: oversampled lengths 2048 and
+4096, the latter with the y-pass twiddles read from global memory).  These
+cases run the operator on the shapes of the 1024x1024x300
 workload (61 tilts, -60..60 step 2) and of the mixed-geometry series (widths
 up to 2048, thickness 100-400, tilt ranges +-45..70 with 1.5-3 degree steps
 and 10% of the tilts dropped), with seeded random inputs, and compare every
@@ -39,6 +41,9 @@ CASES = {
     "2048x400_drop10": (2048, 400, _tilts(-70, 70, 1.5, 0.1, 1), 4),
     "768x100_drop10": (768, 100, _tilts(-45, 45, 3, 0.1, 2), 8),
     "512x257_drop10": (512, 257, _tilts(-55, 62, 2.5, 0.1, 3), 8),
+    # long y rows: n1 = 2048, and n1 = 4096 (twiddles read from global memory)
+    "512x700": (512, 700, _tilts(-60, 60, 3, 0.0, 0), 8),
+    "256x1100": (256, 1100, _tilts(-60, 60, 4, 0.0, 0), 8),
 }
 
 
