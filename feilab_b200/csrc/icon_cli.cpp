@@ -42,7 +42,7 @@ void help()
     printf("-skipCrossValidation (-skipCV) : 1 skips the cross validation and its frc files; default 0.\n######\n");
     printf("-gpu (-g) : the GPUs to use, e.g. 0,2,4,6; default -1, all GPUs.\n######\n");
     printf("-help (-h) : for help.\n");
-    printf("long options: --volume FILE (write the slices as one MRC volume), --batch N (slices per GPU batch)\n");
+    printf("long options: --volume FILE (write the slices as one MRC volume), --batch N (slices per GPU batch, default 128)\n");
 }
 
 struct Args {
@@ -54,7 +54,7 @@ struct Args {
     int thickness = 0;
     int skip_cv = 0;
     std::vector<int> gpus;
-    int batch = 64;
+    int batch = 128;
 };
 
 // Per-GPU work: a contiguous slice range.
