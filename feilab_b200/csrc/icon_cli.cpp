@@ -42,7 +42,8 @@ void help()
     printf("-skipCrossValidation (-skipCV) : 1 skips the cross validation and its frc files; default 0.\n######\n");
     printf("-gpu (-g) : the GPUs to use, e.g. 0,2,4,6; default -1, all GPUs.\n######\n");
     printf("-help (-h) : for help.\n");
-    printf("long options: --volume FILE (write the slices as one MRC volume), --batch N (slices per GPU batch, default 128)\n");
+    printf("long options: --volume FILE (write the slices as one MRC volume), --batch N (slices per GPU batch, default 128),\n"
+           "  --loo (cross-validate every tilt in turn: crossValidation/loo/tiltNNN.frc and loo_summary.txt)\n");
 }
 
 struct Args {
@@ -55,6 +56,7 @@ struct Args {
     int skip_cv = 0;
     std::vector<int> gpus;
     int batch = 128;
+    bool loo = false;
 };
 
 // Per-GPU work: a contiguous slice range.
@@ -209,6 +211,7 @@ int main(int argc, char **argv)
         if (a.size() > 2 && a[0] == '-' && a[1] == '-') {               // long options of this tool
             if (a == "--volume" && next_arg(argc, argv, i, v)) A.volume = v;
             else if (a == "--batch" && next_arg(argc, argv, i, v)) A.batch = std::max(1, atoi(v.c_str()));
+            else if (a == "--loo") { A.loo = true; ++i; }
             else if (a == "--help") { help(); return -1; }
             else { printf("parameter error!\n Please use -help to see the manual\n"); return -1; }
             continue;
@@ -408,6 +411,45 @@ int main(int argc, char **argv)
         };
         write_frc("fullRec.frc", rp_full);
         write_frc("crossV.frc", rp_cv);
+    }
+    if (A.loo) {
+        // Every tilt left out in turn, all the left-out solves in one batched
+        // schedule on the first listed GPU (icon_loo_sweep); per tilt the
+        // smoothed FRC of its reprojections against its projection, written
+        // as crossV.frc is.
+        const int nz = inh.nz, nx = inh.nx;
+        std::vector<float> rows((size_t)slicetotal * nz * nx);
+        for (int s = 0; s < slicetotal; ++s)
+            for (int i = 0; i < nz; ++i)
+                std::memcpy(&rows[((size_t)s * nz + i) * nx], &stack[((size_t)i * inh.ny + A.ystart + s) * nx],
+                            sizeof(float) * nx);
+        icon_solve_cfg cfg{A.iters[0], A.iters[1], A.iters[2], A.data_type, A.threshold};
+        const int half = nx / 2;
+        std::vector<float> frc((size_t)nz * (half > 0 ? half : 1));
+        std::vector<int> iters(nz);
+        if (icon_loo_sweep(rows.data(), nx, thickness, nz, tilts.data(), &cfg, slicetotal, A.batch, 0.0, A.gpus[0],
+                           frc.data(), nullptr, iters.data()) != ICON_OK) {
+            printf("running state: fail!\nError message: leave-one-out sweep: %s\n", icon_last_error());
+            return 1;
+        }
+        const std::string loodir = join(cvdir, "loo");
+        mkdir(loodir.c_str(), 0755);
+        FILE *sum = fopen(join(cvdir, "loo_summary.txt").c_str(), "w");
+        if (sum) fprintf(sum, "# tilt index, angle, mean FRC over the rings, iterations\n");
+        for (int k = 0; k < nz; ++k) {
+            char name[32];
+            snprintf(name, sizeof name, "tilt%03d.frc", k);
+            FILE *f = fopen(join(loodir, name).c_str(), "w");
+            double mean = 0.0;
+            for (int q = 0; q < half; ++q) {
+                if (f) fprintf(f, "%f %f\n", (1.0 / nx) * q, frc[(size_t)k * half + q]);   // as crossV.frc
+                mean += frc[(size_t)k * half + q];
+            }
+            if (f) fclose(f);
+            if (sum) fprintf(sum, "%d %f %f %d\n", k, tilts[k], half > 0 ? mean / half : 0.0, iters[k]);
+        }
+        if (sum) fclose(sum);
+        printf("leave-one-out: %d tilts, FRC files in %s\n", nz, loodir.c_str());
     }
     printf("running state:\n   ICON-GPU finish!\n");
     return 0;

@@ -107,3 +107,36 @@ def test_cli_volume_output(golden, tmp_path):
     for s in range(S):
         _, d = mrc.read(str(out / "reconstruction" / f"mid{s:05d}.mrc"))
         np.testing.assert_array_equal(v[s], d[0])
+
+
+@pytest.mark.gpu
+def test_cli_leave_one_out(golden, tmp_path):
+    # --loo writes one FRC curve per omitted tilt; the curve of the tilt the
+    # reference cross-validates equals the tool's own crossV.frc (the same
+    # left-out solve, run in the batched schedule).
+    from feilab_b200 import mrc
+    from conftest import min_abs_tilt_index
+    z = golden["cli"]
+    nx, th, S = int(z["nx"]), int(z["thickness"]), int(z["S"])
+    nz = len(z["tilts"])
+    stack, tlt, out = tmp_path / "stack.mrc", tmp_path / "cli.tlt", tmp_path / "res"
+    mrc.write_tilt_series(str(stack), z["rows"])
+    mrc.write_tlt(str(tlt), z["tilts"])
+    out.mkdir()
+    a, b, c = (int(v) for v in z["sched"])
+    p = _run(["-i", str(stack), "-t", str(tlt), "-o", str(out), "-s", f"0,{S - 1}", "-iter", f"{a},{b},{c}",
+              "-d", str(int(z["data_type"])), "-thr", str(float(z["threshold"])), "-g", "0", "-thi", str(th),
+              "--loo", "--batch", "8"], str(tmp_path))
+    assert p.returncode == 0, p.stdout + p.stderr
+    cv = out / "crossValidation"
+    files = sorted((cv / "loo").glob("tilt*.frc"))
+    assert len(files) == nz
+    omit = min_abs_tilt_index(z["tilts"])
+    got = np.loadtxt(str(cv / "loo" / f"tilt{omit:03d}.frc"))
+    ref = np.loadtxt(str(cv / "crossV.frc"))
+    np.testing.assert_array_equal(got[:, 0], ref[:, 0])
+    np.testing.assert_allclose(got[:, 1], ref[:, 1], atol=1e-4)
+    summary = np.loadtxt(str(cv / "loo_summary.txt"))
+    assert summary.shape == (nz, 4)
+    np.testing.assert_allclose(summary[:, 1], z["tilts"], atol=1e-5)
+    assert np.all(summary[:, 3] == a + b + c)
