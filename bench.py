@@ -305,7 +305,7 @@ def run_ours(args):
 def warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S):
     """The learned warm start against the plain solve on the same slices:
     timed input stage + network + full schedule (device-resident inputs),
-    the FRC of its result against the plain result (the judge), and the
+    the FRC of its result against the plain result (the acceptance check), and the
     held-out iterations-to-tolerance comparison stored with the weights."""
     import torch
     from feilab_b200 import sharding, warmstart
@@ -335,7 +335,7 @@ def warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S):
     e1.record(stream)
     barrier()
     t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-    # inference alone, and the judge: FRC of the warm result against the cold one
+    # inference alone, and the acceptance check: FRC of the warm result against the cold one
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for s0 in range(0, S, cap):

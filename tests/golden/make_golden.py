@@ -3,7 +3,7 @@
 Run on a machine with a B200 after oracle/build_ref.sh has built
 oracle/_ref/ref_harness and oracle/_ref/ICON-GPU from the reference sources:
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out /tmp/golden
 
 For every case below it writes <case>.npz holding the inputs (tilt angles,
 projection rows, test vectors, iteration schedule) and what the reference's
@@ -112,7 +112,7 @@ def _read_out(path, c):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
     ap.add_argument("--ref", default=os.path.join(ROOT, "oracle", "_ref"))
     ap.add_argument("--cases", default="a,b,c,cli")
     args = ap.parse_args()
