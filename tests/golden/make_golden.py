@@ -9,9 +9,9 @@ For every case below it writes <case>.npz holding the inputs (tilt angles,
 projection rows, test vectors, iteration schedule) and what the reference's
 own routines returned for them (stage outputs of ref_harness).  For the
 "cli" case it also runs the reference ICON-GPU command-line tool on an MRC
-tilt series and keeps its output files.  The npz files are then copied into
-tests/golden/ and committed; tests compare the oracle and the CUDA path with
-them.  Inputs are generated here once, so the tests never regenerate them.
+tilt series and keeps its output files.  The npz files go to tests/golden/
+by default, where they are committed; tests compare the oracle and the CUDA
+path with them.  Inputs are generated here once, so the tests never regenerate them.
 """
 from __future__ import annotations
 
