@@ -11,16 +11,24 @@
 // fixed size, so the only memory it touches besides the caller's input and
 // output is that array.
 //
-// The array is a static of this library: every GPU that loads the library
-// holds its ICON_NOALLOC_SCRATCH_BYTES from module load until the process
-// exits.  All calls share it and it keeps the last call's contents; every
+// The array is a static of this library's device code.  It is allocated when
+// the library's device code is loaded on a GPU and stays until the process
+// exits.  With lazy module loading (the CUDA default since 12.2) that load
+// happens at the first use of the library's device code on each device --
+// for a caller of this entry point alone, its first call there -- and the
+// load allocates device memory and may synchronise.  So make the first call
+// on each device before a pool allocator takes the device's memory and before
+// any real-time region or stream capture, or run with
+// CUDA_MODULE_LOADING=EAGER, which loads it when the context is created.
+// Later calls allocate nothing.
+//
+// All calls share the array and it keeps the last call's contents; every
 // call rewrites all of the tables it reads, so nothing in it has to start at
 // zero.  Calls that overlap on a GPU (different streams, or different host
 // threads) race on the array and must not be issued.
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 #include <string>
 
 #include "icon_b200.h"
@@ -28,7 +36,6 @@
 
 namespace {
 
-constexpr int kMaxDevices = 64;
 constexpr int kNx = ICON_NOALLOC_MAX_NX;
 constexpr int kN = 2 * ICON_NOALLOC_MAX_NX;   // largest oversampled length, 2*nextpow2(nx)
 
@@ -41,9 +48,6 @@ constexpr size_t kEnd = kOffTw + sizeof(float2) * kN;
 static_assert(kEnd <= ICON_NOALLOC_SCRATCH_BYTES, "scratch array too small for its tables");
 
 __device__ __align__(256) unsigned char g_scratch[ICON_NOALLOC_SCRATCH_BYTES];
-
-std::mutex g_mu;
-unsigned char *g_scratch_addr[kMaxDevices];   // device address of g_scratch, per device
 
 }  // namespace
 
@@ -136,22 +140,20 @@ __global__ void __launch_bounds__(1024) k_na_rows(const unsigned char *__restric
     }
 }
 
-// Once per device, with that device current: the device address of the
-// scratch array (host code cannot use the symbol itself as a pointer) and the
-// shared-memory limit of the row kernel.
-icon_status device_setup(int dev, unsigned char **out)
+// On every call, with the device current: the device address of the scratch
+// array in the current context (host code cannot use the symbol itself as a
+// pointer) and the shared-memory limit of the row kernel.  Both are looked up
+// again each time rather than cached, so a context that was reset
+// (cudaDeviceReset) and recreated, with the module loaded anew, is handled;
+// neither call allocates once the module is loaded.
+icon_status device_setup(unsigned char **out)
 {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (dev < 0 || dev >= kMaxDevices) return na_fail(ICON_ERR_INVALID, "device ordinal out of range");
-    if (!g_scratch_addr[dev]) {
-        void *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_scratch);
-        if (e != cudaSuccess) return na_fail(ICON_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        e = cudaFuncSetAttribute(k_na_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * (int)sizeof(float2));
-        if (e != cudaSuccess) return na_fail(ICON_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-        g_scratch_addr[dev] = (unsigned char *)ptr;
-    }
-    *out = g_scratch_addr[dev];
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_scratch);
+    if (e != cudaSuccess) return na_fail(ICON_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    e = cudaFuncSetAttribute(k_na_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * (int)sizeof(float2));
+    if (e != cudaSuccess) return na_fail(ICON_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    *out = (unsigned char *)ptr;
     return ICON_OK;
 }
 
@@ -163,11 +165,8 @@ extern "C" icon_status icon_rows_forward_noalloc(const float *d_rows, int nx, in
     if (nx < 8 || nx > ICON_NOALLOC_MAX_NX)
         return na_fail(ICON_ERR_INVALID, "nx must be in [8, " + std::to_string(ICON_NOALLOC_MAX_NX) + "]");
     if (ntilt < 1 || S < 1) return na_fail(ICON_ERR_INVALID, "ntilt and S must be >= 1");
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return na_fail(ICON_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     unsigned char *scr = nullptr;
-    icon_status rc = device_setup(dev, &scr);
+    icon_status rc = device_setup(&scr);
     if (rc != ICON_OK) return rc;
     // Grid of the reference: n = 2*nextpow2(nx), window parameters in float
     // (MainCode.cu:66-71, NU:1330-1331).
@@ -186,7 +185,7 @@ extern "C" icon_status icon_rows_forward_noalloc(const float *d_rows, int nx, in
     k_na_tables<<<(n + 255) / 256, 256, 0, st>>>(scr, nx, n, b, bf);
     k_na_rows<<<dim3(ntilt, G), n * B / 16, (size_t)n * B * sizeof(float2), st>>>(scr, d_rows, (float2 *)d_b, nx, ntilt, n,
                                                                                   lg, S, B);
-    e = cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return na_fail(ICON_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     return ICON_OK;
 }

@@ -52,6 +52,22 @@ struct Plan {
     ~Plan() { icon_plan_destroy(p); }
 };
 
+// Makes `dev` current for the sweep and gives the calling thread its previous
+// device back on every return path.
+struct CurrentDevice {
+    int prev = -1;
+    bool ok = false;
+    explicit CurrentDevice(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~CurrentDevice()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 }  // namespace
 
 extern "C" icon_status icon_loo_sweep(const float *h_rows, int nx, int thickness, int nz, const float *tilt_deg,
@@ -60,7 +76,8 @@ extern "C" icon_status icon_loo_sweep(const float *h_rows, int nx, int thickness
 {
     if (!h_rows || !tilt_deg || !cfg || !h_frc || nx < 2 || thickness < 1 || nz < 3 || S < 1 || capacity < 1)
         return loo_fail(ICON_ERR_INVALID, "icon_loo_sweep: bad argument");
-    if (cudaSetDevice(device) != cudaSuccess) return loo_fail(ICON_ERR_CUDA, "icon_loo_sweep: cudaSetDevice");
+    CurrentDevice cur(device);
+    if (!cur.ok) return loo_fail(ICON_ERR_CUDA, "icon_loo_sweep: cudaSetDevice");
     icon_status rc = ICON_OK;
     // One plan over all tilts; its capacity bounds a batch.
     const int cap = capacity;

@@ -111,7 +111,8 @@ int *device_err_flag()
 // Launches one convolution; used by the network code and exported for tests.
 icon_status ws_conv3x3_launch(const void *in0, int cin0, const void *in1, int cin1, int nimg, int H, int W,
                               const void *w, const float *bias, int N, int relu, void *out0, int nsplit, int acc0,
-                              void *out1, int acc1, cudaStream_t st)
+                              void *out1, int acc1, cudaStream_t st, unsigned long long wait_ns = ws::kWaitNs,
+                              int hold = 0)
 {
     if (!in0 || !w || !out0 || nimg < 1 || H < 1 || W < 1) return ws_fail(ICON_ERR_INVALID, "conv3x3: bad argument");
     if (N < 16 || N > 256 || N % 16) return ws_fail(ICON_ERR_INVALID, "conv3x3: N must be a multiple of 16 in 16..256");
@@ -144,6 +145,8 @@ icon_status ws_conv3x3_launch(const void *in0, int cin0, const void *in1, int ci
     a.bias = bias;
     a.relu = relu;
     a.err = err;
+    a.wait_ns = wait_ns;
+    a.hold = hold;
     const size_t smem = ws::conv_smem_bytes(N, cc);
     {
         // The shared-memory limit is a per-device attribute of the kernel.
@@ -172,6 +175,14 @@ icon_status icon_ws_conv3x3(const void *in0, int cin0, const void *in1, int cin1
 {
     return ws_conv3x3_launch(in0, cin0, in1, cin1, nimg, H, W, w, bias, N, relu, out0, nsplit, acc0, out1, acc1,
                              (cudaStream_t)stream);
+}
+
+icon_status icon_ws_conv3x3_wait_test(const void *in0, int cin0, int nimg, int H, int W, const void *w, int N,
+                                      void *out0, unsigned wait_us, void *stream)
+{
+    if (wait_us < 1 || wait_us > 1000000) return ws_fail(ICON_ERR_INVALID, "wait_us must be in 1..1000000");
+    return ws_conv3x3_launch(in0, cin0, nullptr, 0, nimg, H, W, w, nullptr, N, 0, out0, N, 0, nullptr, 0,
+                             (cudaStream_t)stream, 1000ull * wait_us, 1);
 }
 
 icon_status icon_ws_device_error(int *h_code)

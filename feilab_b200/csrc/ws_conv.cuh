@@ -38,6 +38,13 @@ struct ConvArgs {
     const float *bias;       // [N] or null
     int relu;
     int *err;                // device error flag
+    // Limit of the pipeline's load and MMA waits (normally kWaitNs).  The
+    // waits that drain copies and MMAs before the CTA exits always use
+    // kWaitNs, so nothing is left in flight.
+    unsigned long long wait_ns;
+    // Test of the bounded waits: the first stage's barrier expects 16 bytes
+    // more than its loads deliver, so the wait for it can only run out.
+    int hold;
 };
 
 __host__ __device__ inline size_t conv_stage_a_bytes(int cc) { return (size_t)kTileM * cc * 2; }
@@ -106,7 +113,7 @@ k_conv3x3_tc(const __grid_constant__ CUtensorMap in0, const __grid_constant__ CU
                 const bool second = g >= chunks0;
                 const int c0 = (second ? g - chunks0 : g) * a.cc;
                 const int wc0 = (second ? a.cin0 : 0) + c0;
-                mbar_expect_tx(&full[s], tx);
+                mbar_expect_tx(&full[s], tx + ((a.hold && k == 0) ? 16u : 0u));
                 tma_load_4d(sa + s * abytes, second ? &in1 : &in0, c0, w0 + dx - 1, h + dy - 1, img, &full[s]);
                 tma_load_3d(sb + s * bbytes, &wmap, wc0, 0, tap, &full[s]);
             };
@@ -115,7 +122,7 @@ k_conv3x3_tc(const __grid_constant__ CUtensorMap in0, const __grid_constant__ CU
             int issued = pre;
             for (int k = 0; k < steps && ok; ++k) {
                 const int s = k % kConvStages;
-                if (!mbar_wait(&full[s], (uint32_t)((k / kConvStages) & 1), a.err, kErrLoadWait)) {
+                if (!mbar_wait(&full[s], (uint32_t)((k / kConvStages) & 1), a.err, kErrLoadWait, a.wait_ns)) {
                     ok = false;
                     break;
                 }
@@ -131,7 +138,7 @@ k_conv3x3_tc(const __grid_constant__ CUtensorMap in0, const __grid_constant__ CU
                 // k's MMAs stay queued meanwhile).
                 if (k >= 1 && issued < steps) {
                     const int kp = k - 1, sp = kp % kConvStages;
-                    if (!mbar_wait(&empty[sp], (uint32_t)((kp / kConvStages) & 1), a.err, kErrMmaWait)) {
+                    if (!mbar_wait(&empty[sp], (uint32_t)((kp / kConvStages) & 1), a.err, kErrMmaWait, a.wait_ns)) {
                         ok = false;
                         break;
                     }

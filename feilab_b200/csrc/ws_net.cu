@@ -32,7 +32,8 @@
 extern "C" void icon_internal_set_error(const char *msg);
 icon_status ws_conv3x3_launch(const void *in0, int cin0, const void *in1, int cin1, int nimg, int H, int W,
                               const void *w, const float *bias, int N, int relu, void *out0, int nsplit, int acc0,
-                              void *out1, int acc1, cudaStream_t st);
+                              void *out1, int acc1, cudaStream_t st, unsigned long long wait_ns = 2000000000ull,
+                              int hold = 0);
 
 namespace {
 

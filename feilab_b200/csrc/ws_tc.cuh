@@ -56,13 +56,14 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
 }
 
 // Waits for the phase with the given parity to complete; false (and *err set
-// to code) when kWaitNs passes first.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code)
+// to code) when limit_ns passes first.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code,
+                                          unsigned long long limit_ns = kWaitNs)
 {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (!mbar_try(bar, parity)) {
-        if (global_ns() - t0 > kWaitNs) {
+        if (global_ns() - t0 > limit_ns) {
             atomicCAS(err, kErrNone, code);
             return false;
         }

@@ -24,6 +24,8 @@ def lib():
         L.icon_ws_conv3x3.restype = ctypes.c_int
         L.icon_ws_device_error.argtypes = [ctypes.POINTER(I)]
         L.icon_ws_device_error.restype = ctypes.c_int
+        L.icon_ws_conv3x3_wait_test.argtypes = [V, I, I, I, I, V, I, V, ctypes.c_uint, V]
+        L.icon_ws_conv3x3_wait_test.restype = ctypes.c_int
         F, D, Z = ctypes.c_float, ctypes.c_double, ctypes.c_size_t
         L.icon_ws_create.argtypes = [P, I, ctypes.POINTER(P)]
         L.icon_ws_destroy.argtypes = [P]
@@ -83,6 +85,18 @@ def conv3x3(in0, w, bias=None, relu=False, in1=None, nsplit=None, out0=None, out
     _check(lib().icon_ws_conv3x3(_ptr(in0), c0, _ptr(in1), c1, n, H, W, _ptr(w), _ptr(bias), N, int(relu),
                                  _ptr(out0), nsplit, int(acc0), _ptr(out1), int(acc1), _stream()))
     return (out0, out1) if nsplit < N else out0
+
+
+def conv3x3_wait_test(in0, w, wait_us):
+    """icon_ws_conv3x3_wait_test: a convolution whose first pipeline stage
+    can never complete, so its bounded wait runs out after wait_us
+    microseconds; returns the (skipped) output tensor."""
+    import torch
+    n, H, W, c0 = in0.shape
+    N = w.shape[1]
+    out0 = torch.zeros((n, H, W, N), dtype=torch.bfloat16, device=in0.device)
+    _check(lib().icon_ws_conv3x3_wait_test(_ptr(in0), c0, n, H, W, _ptr(w), N, _ptr(out0), int(wait_us), _stream()))
+    return out0
 
 
 def param_count() -> int:

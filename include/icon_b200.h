@@ -253,12 +253,18 @@ long long icon_launch_count(const icon_plan *plan);
  * can block on the device -- and so cannot create a plan.  No counterpart in
  * the reference.  It calls no cudaMalloc, cudaFree or allocating library
  * routine: its tables live in one file-scope __device__ array of
- * ICON_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until
- * the process exits.  nx must be in [8, ICON_NOALLOC_MAX_NX] (larger sizes
- * return ICON_ERR_INVALID).  Runs on the current device and on `stream`.  The
- * first call on a device looks up the array's device address and sets a
- * kernel attribute, so make that first call before any stream capture.  All
- * calls share the array: calls that overlap on one GPU (other streams or host
+ * ICON_NOALLOC_SCRATCH_BYTES, part of this library's device code.  That code
+ * is loaded on a device, the array with it, at the first use of the library
+ * there under lazy module loading (the CUDA default since 12.2; with
+ * CUDA_MODULE_LOADING=EAGER, at context creation), and the load allocates
+ * device memory and may synchronise: make the first call on each device
+ * before a pool allocator takes its memory, before any real-time region and
+ * before any stream capture.  The array then stays until the process exits;
+ * later calls allocate nothing.  Every call looks up the array's device
+ * address and sets the row kernel's shared-memory limit (cheap host calls).
+ * nx must be in [8, ICON_NOALLOC_MAX_NX] (larger sizes return
+ * ICON_ERR_INVALID).  Runs on the current device and on `stream`.  All calls
+ * share the array: calls that overlap on one GPU (other streams or host
  * threads) race on it and must be serialised by the caller. */
 #define ICON_NOALLOC_MAX_NX 4096
 #define ICON_NOALLOC_SCRATCH_BYTES (512 * 1024)

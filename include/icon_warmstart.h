@@ -82,6 +82,17 @@ icon_status icon_ws_update(icon_ws *ws, float lr, void *stream);
 icon_status icon_ws_train_step(icon_ws *ws, const void *d_Ahwb, const float *d_target, int S, float lr,
                                double *h_loss, void *stream);
 
+/* Test of the convolution's bounded waits (no reference counterpart): one
+ * convolution as icon_ws_conv3x3 (one input, no bias, no ReLU, one output)
+ * whose first pipeline stage waits for 16 bytes more than its loads deliver,
+ * so that the wait for it ends only by running out after wait_us
+ * microseconds (1 .. 1000000).  The kernel then records error code 1, lets
+ * the loads it issued land (within 2 s), skips its output, releases its
+ * tensor memory and returns; icon_ws_device_error reports the code and the
+ * device stays usable. */
+icon_status icon_ws_conv3x3_wait_test(const void *in0, int cin0, int nimg, int H, int W, const void *w, int N,
+                                      void *out0, unsigned wait_us, void *stream);
+
 /* Reads and clears the current device's error flag of the tensor-core
  * kernels (0: none; 1, 2, 3: a bounded wait for a TMA load, for the MMAs of
  * a stage, or for the accumulator ran out; the kernel then skipped its

@@ -3,7 +3,7 @@
 Run on a machine with a B200 after oracle/build_ref.sh has built
 oracle/_ref/ref_harness and oracle/_ref/ICON-GPU from the reference sources:
 
-    python tests/golden/make_golden.py --out /tmp/golden
+    python tests/golden/make_golden.py [--out DIR] [--cases a,b,c,cli]
 
 For every case below it writes <case>.npz holding the inputs (tilt angles,
 projection rows, test vectors, iteration schedule) and what the reference's

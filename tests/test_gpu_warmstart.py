@@ -88,6 +88,26 @@ def test_conv3x3_repeatable():
     assert torch.equal(a, b)
 
 
+def test_conv3x3_bounded_wait_runs_out_and_device_stays_usable():
+    # A stage barrier that can never complete (it expects 16 bytes more than
+    # its loads deliver): the wait gives up after 1 ms, the kernel records
+    # code 1 (load wait), lets its copies land, skips its output and returns;
+    # the next convolution on the device is correct.
+    from feilab_b200 import warmstart
+    g = torch.Generator(device="cuda").manual_seed(11)
+    x = torch.randn((1, 2, 128, 32), generator=g, device="cuda").to(torch.bfloat16)
+    w = (torch.randn((9, 32, 32), generator=g, device="cuda") / 17).to(torch.bfloat16)
+    assert warmstart.device_error() == 0
+    out = warmstart.conv3x3_wait_test(x, w, 1000)
+    torch.cuda.synchronize()
+    assert warmstart.device_error() == 1
+    assert not out.float().abs().any()          # the output was skipped
+    again = warmstart.conv3x3(x, w)
+    torch.cuda.synchronize()
+    assert warmstart.device_error() == 0
+    _close(again, _ref_conv(x, None, w, None, False))
+
+
 def test_conv3x3_rejects_bad_shapes():
     from feilab_b200 import warmstart
     from feilab_b200.icon import IconError
