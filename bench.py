@@ -21,8 +21,19 @@ data path).
 --impl reference: the reference has no CPU implementation of this path, so
 the CPU arm is the oracle's float port of it (oracle/icon_oracle_core.c, the
 reference's own algorithm restated in C, OpenMP over slices on all host
-cores) on a bounded sample of the same workload, extrapolated to 300
-iterations.
+cores) on a bounded sample of the same workload: one slice per host thread,
+the 300-iteration schedule cut into 20 pieces of 15 iterations (the input
+stage goes with the first), one piece per step, the image carried from step
+to step, so 20 steps run one whole reconstruction of the sample.  value =
+slices x (steps / 20) / measured time.  The repo arm's cpu_baseline runs the
+same sample through all 20 pieces, timed as a whole.
+
+Also in the repo arm's line: reference_gpu (the reference's own ICON-GPU,
+compiled from its sources for sm_100a into oracle/_ref/, run by wall clock
+on a 64-slice stack of the workload, and the agreement of its slices with
+this build's) and parity (this build's result on the 16 slices of
+tests/golden/cfg2.npz against the reference's and the FP64 oracle's results
+for the same 300 iterations).
 """
 from __future__ import annotations
 
@@ -128,50 +139,179 @@ def make_rows(ys, device):
     return rows, tilts
 
 
-def cpu_sample(tilts, rows_np, nthreads=0):
-    """Oracle float port on a bounded sample: S_cpu slices (one per thread),
-    input stage alone, then input stage + 3 iterations; slices/s extrapolated
-    to the full 300-iteration schedule."""
-    from oracle.oracle import OraclePlan
-    p = OraclePlan(NX, THICK, tilts, "f32")
-    S = rows_np.shape[0]
-    t0 = time.perf_counter()
-    p.reconstruct(rows_np, (0, 0, 0), DATA_TYPE, THRESHOLD, nthreads=nthreads)
-    t_rhs = time.perf_counter() - t0
-    k = 3
-    t0 = time.perf_counter()
-    p.reconstruct(rows_np, (0, k, 0), DATA_TYPE, THRESHOLD, nthreads=nthreads)
-    t_k = time.perf_counter() - t0
-    per_iter = max(t_k - t_rhs, 1e-9) / k
-    t_full = t_rhs + per_iter * sum(SCHED)
-    return S / t_full, p.threads_used, dict(t_rhs=t_rhs, t_3iter=t_k, per_iter=per_iter)
+NPIECES, PIECE_ITERS = 20, 15    # the 300-iteration schedule in timed pieces
+
+
+def schedule_piece(k, sched=SCHED, per=PIECE_ITERS):
+    """(INFR before, ICON, INFR after) counts of iterations [k*per, (k+1)*per)
+    of the schedule (Iteration2.cu:129-132)."""
+    a, b, c = sched
+    lo, hi = k * per, (k + 1) * per
+
+    def ov(x0, x1):
+        return max(0, min(hi, x1) - max(lo, x0))
+    return ov(0, a), ov(a, a + b), ov(a + b, a + b + c)
+
+
+class CpuSchedule:
+    """The oracle's float port on a sample of slices (OpenMP over slices), run
+    piece by piece: step() runs the next piece of the schedule (piece 0 starts
+    with the input stage and m = 0); the image is carried between pieces, so
+    NPIECES steps make one whole reconstruction; then the next step starts a
+    new one."""
+
+    def __init__(self, tilts, rows_np, nthreads=0):
+        from oracle.oracle import OraclePlan
+        self.p = OraclePlan(NX, THICK, tilts, "f32")
+        self.rows = np.ascontiguousarray(rows_np, np.float32)
+        self.S = self.rows.shape[0]
+        self.nthreads = nthreads
+        self.k = 0
+        self.A = self.m = None
+
+    def step(self):
+        if self.k == 0:
+            self.A = self.p.rhs_batch(self.rows, self.nthreads)
+            self.m = np.zeros((self.S, NX, THICK), np.float32)
+        self.p.solve_batch(self.A, self.m, schedule_piece(self.k), DATA_TYPE, THRESHOLD, self.nthreads)
+        self.k = (self.k + 1) % NPIECES
+
+    @property
+    def threads(self):
+        return self.p.threads_used
+
+
+def cpu_rows(tilts, rows_dev=None):
+    """One slice per host thread: the first slices of the workload."""
+    ncpu = os.cpu_count() or 1
+    if rows_dev is not None:
+        return rows_dev.reshape(-1, len(tilts), NX)[:ncpu].cpu().numpy()
+    rows, _ = make_rows(list(range(ncpu)), "cpu")
+    return rows.numpy()
 
 
 def run_reference(args):
-    import torch
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    ncpu = os.cpu_count() or 1
-    ys = list(range(0, NY, max(1, NY // ncpu)))[:ncpu]
-    rows, tilts = make_rows(ys, "cpu")
-    rows_np = rows.numpy()
-    vals = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        v, used, info = cpu_sample(tilts, rows_np)
-        if i >= args.warmup:
-            vals.append(v)
-    value = float(np.mean(vals))
-    sample = (f"{len(ys)} slices of the workload per step (one per host thread), input stage + 3 iterations timed, "
-              f"extrapolated to {sum(SCHED)} iterations (per-iteration {info['per_iter']:.3f} s/slice-batch)")
+    from feilab_b200 import synth
+    tilts = synth.tilt_angles(-60, 60, 2)
+    rows_np = cpu_rows(tilts)
+    cs = CpuSchedule(tilts, rows_np)
+    for _ in range(args.warmup):
+        cs.step()
+    cs.k = 0                                   # the timed steps start a reconstruction
+    times = []
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cs.step()
+        times.append(time.perf_counter() - t0)
+    total = time.perf_counter() - t_all
+    value = cs.S * (args.steps / NPIECES) / total
+    sample = (f"{cs.S} slices of the workload (one per host thread); step i runs iterations "
+              f"{PIECE_ITERS}*(i mod {NPIECES}) .. +{PIECE_ITERS} of the {sum(SCHED)}-iteration schedule "
+              f"(the input stage with the first), the image carried between steps; {args.steps} timed steps = "
+              f"{args.steps / NPIECES:g} reconstructions of the sample; value = slices x steps/{NPIECES} / measured time")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "slices/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": len(ys) / value * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+            "ms_per_step_minmax": [round(min(times) * 1e3, 1), round(max(times) * 1e3, 1)],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "implementation": "oracle float port of the reference algorithm (no CPU build of the path exists in the reference)"},
-            "cpu_baseline": {"value": value, "unit": "slices/s", "cores": used, "kind": "port", "sample": sample},
+            "config": {"workload": WORKLOAD, "implementation": "oracle float port of the reference algorithm "
+                       "(no CPU build of the path exists in the reference)"},
+            "cpu_baseline": {"value": value, "unit": "slices/s", "cores": cs.threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_full(tilts, rows_np):
+    """One whole reconstruction (input stage + 300 iterations) of one slice per
+    host thread by the oracle's float port, timed as a whole."""
+    cs = CpuSchedule(tilts, rows_np)
+    t0 = time.perf_counter()
+    for _ in range(NPIECES):
+        cs.step()
+    t = time.perf_counter() - t0
+    return {"value": cs.S / t, "unit": "slices/s", "cores": cs.threads, "kind": "port",
+            "seconds": round(t, 2),
+            "sample": f"{cs.S} slices of the workload (one per host thread), input stage + all {sum(SCHED)} "
+                      f"iterations, measured wall time"}
+
+
+def reference_gpu_leg(tilts, rows_dev, plan, nslices=64):
+    """The reference ICON-GPU (oracle/_ref/ICON-GPU, built from the reference
+    sources for sm_100a) on an MRC stack of `nslices` slices of the workload,
+    -iter 10,280,10 -d 2 -thr 0 -thi 300 -skipCV 1 -g 0, timed by wall clock
+    around the process; its slice files against this build's slices."""
+    from feilab_b200 import mrc
+    exe = os.path.join(ROOT, "oracle", "_ref", "ICON-GPU")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ICON-GPU not built (oracle/build_ref.sh needs the reference sources)"}
+    rows = rows_dev[:nslices].contiguous()
+    rows_np = rows.cpu().numpy()
+    with tempfile.TemporaryDirectory() as d:
+        stack, tlt, out = os.path.join(d, "stack.mrc"), os.path.join(d, "s.tlt"), os.path.join(d, "out")
+        os.makedirs(out)
+        mrc.write_tilt_series(stack, rows_np)
+        mrc.write_tlt(tlt, tilts)
+        a, b, c = SCHED
+        cmd = [exe, "-i", stack, "-t", tlt, "-o", out, "-s", f"0,{nslices - 1}", "-iter", f"{a},{b},{c}",
+               "-d", str(DATA_TYPE), "-thr", str(THRESHOLD), "-g", "0", "-thi", str(THICK), "-skipCV", "1"]
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd, capture_output=True, text=True)
+        wall = time.perf_counter() - t0
+        if p.returncode != 0:
+            return {"unavailable": f"ICON-GPU exited with {p.returncode}: {p.stderr[-200:]}"}
+        per = []
+        for line in p.stdout.splitlines():
+            if line.startswith("slice") and "finished" in line and "time" in line:
+                try:
+                    per.append(float(line.rsplit("time", 1)[1].strip()))
+                except ValueError:
+                    pass
+        ref = np.stack([mrc.read(os.path.join(out, "reconstruction", f"mid{y:05d}.mrc"))[1][0].T
+                        for y in range(nslices)])            # (S, N0, N1), Y fastest
+    A = plan.prepare_rhs(rows)
+    ours = plan.solve(A, SCHED, DATA_TYPE, THRESHOLD).cpu().numpy()
+    rel = [float(np.linalg.norm(ours[s] - ref[s]) / max(np.linalg.norm(ref[s]), 1e-30)) for s in range(nslices)]
+    res = {"value": nslices / wall, "unit": "slices/s", "slices": nslices, "wall_s": round(wall, 2),
+           "command": "ICON-GPU -s 0,%d -iter %d,%d,%d -d %d -thr %g -g 0 -thi %d -skipCV 1" %
+                      (nslices - 1, a, b, c, DATA_TYPE, THRESHOLD, THICK),
+           "rel_l2_vs_this_build_max": max(rel), "rel_l2_vs_this_build_mean": float(np.mean(rel))}
+    if per:
+        res["solve_s_per_slice_mean"] = float(np.mean(per))
+        res["value_solve_only"] = 1.0 / float(np.mean(per))
+    return res
+
+
+def parity_leg(plan_factory):
+    """This build's reconstruction of the 16 slices of tests/golden/cfg2.npz
+    (seeded random slices of the workload, full schedule) against the
+    reference's result (ref_harness) and the FP64 oracle's, same iterations."""
+    import torch
+    from feilab_b200.train_warmstart import frc_mean
+    path = os.path.join(ROOT, "tests", "golden", "cfg2.npz")
+    if not os.path.exists(path):
+        return {"unavailable": "tests/golden/cfg2.npz not present"}
+    z = np.load(path)
+    S = int(z["S"])
+    plan = plan_factory(S)
+    rows = torch.from_numpy(np.ascontiguousarray(z["rows"])).cuda()
+    m = plan.solve(plan.prepare_rhs(rows), tuple(int(v) for v in z["sched"]), int(z["data_type"]),
+                   float(z["threshold"])).cpu()
+    plan.close()
+    m64 = torch.from_numpy(z["m_fp64"].astype(np.float32))
+    mref = torch.from_numpy(z["ref_m"].astype(np.float32))
+
+    def rel(a, b):
+        return [float(((a[s].double() - b[s].double()).norm() / b[s].double().norm()).item()) for s in range(S)]
+    r64, rref = rel(m, m64), rel(m, mref)
+    return {"slices": S, "iterations": int(sum(int(v) for v in z["sched"])), "y": z["ys"].tolist(),
+            "rel_l2_vs_fp64_max": max(r64), "rel_l2_vs_fp64_mean": float(np.mean(r64)),
+            "frc_vs_fp64_min": float(frc_mean(m, m64).min()),
+            "rel_l2_vs_reference_max": max(rref), "rel_l2_vs_reference_mean": float(np.mean(rref)),
+            "frc_vs_reference_min": float(frc_mean(m, mref).min()),
+            "reference_vs_fp64_max": max(rel(mref, m64))}
 
 
 def run_ours(args):
@@ -288,13 +428,14 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "clocks": clocks}
     line["warm_start"] = warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S)
+    if rank == 0:
+        line["parity"] = parity_leg(lambda n: icon.IconPlan(NX, THICK, tilts, capacity=n, device=local))
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu_leg(tilts, rows[0], plan)
+        if "value" in line["reference_gpu"]:
+            line["reference_gpu"]["speedup_e2e"] = round(e2e / line["reference_gpu"]["value"], 2)
     if rank == 0 and world == 1 and not args.no_cpu:
-        ncpu = os.cpu_count() or 1
-        rows_cpu = rows.view(-1, len(tilts), NX)[:ncpu].cpu().numpy()
-        v, used, info = cpu_sample(tilts, rows_cpu)
-        line["cpu_baseline"] = {"value": v, "unit": "slices/s", "cores": used, "kind": "port",
-                                "sample": f"{rows_cpu.shape[0]} slices (one per host thread), input stage + 3 iterations, "
-                                          f"extrapolated to {sum(SCHED)} iterations"}
+        line["cpu_baseline"] = cpu_baseline_full(tilts, cpu_rows(tilts, rows))
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
@@ -383,6 +524,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference ICON-GPU leg")
     ap.add_argument("--profile", action="store_true", help="run the small ncu case only")
     args = ap.parse_args()
     if args.profile:

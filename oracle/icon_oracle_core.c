@@ -586,6 +586,58 @@ int FN(ora_reconstruct)(const void *pp, const float *rows, int S, int a, int bmi
 
 /* Direct NDFT in double (known-answer check, no reference counterpart):
  * f_j = sum_{X,Y} img[X][Y] exp(-2 pi i ((X-N0/2) x0_j + (Y-N1/2) x1_j)). */
+/* Batched input stage and solve for timing the CPU path in pieces: S slices,
+ * OpenMP over slices.  ora_rhs_batch: Ahwb[s] = A^H W b of rows[s] (the input
+ * stage of Lib_2D2, MainCode.cu:115-134).  ora_solve_batch: ora_solve on every
+ * slice, m[s] holding its start value on entry, so that consecutive calls
+ * with consecutive pieces of the schedule (a, bmid, c counted within each
+ * piece) run the whole schedule: the iteration carries no state but m.
+ * Return the number of threads used. */
+int FN(ora_rhs_batch)(const void *pp, const float *rows, int S, REAL *Ahwb, int nthreads)
+{
+    const ora_plan *p = (const ora_plan *)pp;
+    size_t NN = (size_t)p->N0 * p->N1, R = (size_t)p->nz * p->nx;
+    int used = 1;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+    {
+#pragma omp single
+        used = omp_get_num_threads();
+#pragma omp for schedule(dynamic, 1)
+        for (int s = 0; s < S; s++) FN(ora_rhs)(pp, rows + (size_t)s * R, Ahwb + (size_t)s * 2 * NN);
+    }
+#else
+    (void)nthreads;
+    for (int s = 0; s < S; s++) FN(ora_rhs)(pp, rows + (size_t)s * R, Ahwb + (size_t)s * 2 * NN);
+#endif
+    return used;
+}
+
+int FN(ora_solve_batch)(const void *pp, const REAL *Ahwb, int S, int a, int bmid, int c, int dataType,
+                        float threshold, REAL *m, int nthreads)
+{
+    const ora_plan *p = (const ora_plan *)pp;
+    size_t NN = (size_t)p->N0 * p->N1;
+    int used = 1;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+    {
+#pragma omp single
+        used = omp_get_num_threads();
+#pragma omp for schedule(dynamic, 1)
+        for (int s = 0; s < S; s++)
+            FN(ora_solve)(pp, Ahwb + (size_t)s * 2 * NN, a, bmid, c, dataType, threshold, m + (size_t)s * NN, NULL, NULL);
+    }
+#else
+    (void)nthreads;
+    for (int s = 0; s < S; s++)
+        FN(ora_solve)(pp, Ahwb + (size_t)s * 2 * NN, a, bmid, c, dataType, threshold, m + (size_t)s * NN, NULL, NULL);
+#endif
+    return used;
+}
+
 void FN(ora_ndft_forward)(const void *pp, const double *img, int img_is_real, double *f)
 {
     const ora_plan *p = (const ora_plan *)pp;

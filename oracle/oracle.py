@@ -61,6 +61,10 @@ def _declare(L):
         getattr(L, "ora_reproject" + sfx).argtypes = [_P, _P, _P, _P]
         getattr(L, "ora_reconstruct" + sfx).argtypes = [_P, _P, _I, _I, _I, _I, _I, _F, _P, _I]
         getattr(L, "ora_reconstruct" + sfx).restype = _I
+        getattr(L, "ora_rhs_batch" + sfx).argtypes = [_P, _P, _I, _P, _I]
+        getattr(L, "ora_rhs_batch" + sfx).restype = _I
+        getattr(L, "ora_solve_batch" + sfx).argtypes = [_P, _P, _I, _I, _I, _I, _I, _F, _P, _I]
+        getattr(L, "ora_solve_batch" + sfx).restype = _I
         getattr(L, "ora_ndft_forward" + sfx).argtypes = [_P, _P, _I, _P]
         getattr(L, "ora_ndft_adjoint" + sfx).argtypes = [_P, _P, _P]
     L.ora_grid_params.argtypes = [_I, fp, ctypes.POINTER(_I), fp, fp]
@@ -193,6 +197,23 @@ class OraclePlan:
         a, b, c = iters
         used = self._fn("ora_reconstruct")(self._h, _ptr(r), S, a, b, c, data_type, ctypes.c_float(threshold), _ptr(m), nthreads)
         self.threads_used = used
+        return m
+
+    def rhs_batch(self, rows: np.ndarray, nthreads=0) -> np.ndarray:
+        """rows (S, nz, nx) -> A^H W b (S, N0, N1); OpenMP over slices."""
+        r = np.ascontiguousarray(rows, dtype=np.float32)
+        out = np.zeros((r.shape[0], self.N0, self.N1), self.cplx)
+        self.threads_used = self._fn("ora_rhs_batch")(self._h, _ptr(r), r.shape[0], _ptr(out), nthreads)
+        return out
+
+    def solve_batch(self, Ahwb, m, iters, data_type, threshold, nthreads=0):
+        """ICON iterations (a, b, c) on every slice, in place: m (S, N0, N1)
+        holds the start values and receives the results; OpenMP over slices."""
+        A = np.ascontiguousarray(Ahwb, dtype=self.cplx)
+        assert m.dtype == self.real and m.flags["C_CONTIGUOUS"] and m.shape == A.shape
+        a, b, c = iters
+        self.threads_used = self._fn("ora_solve_batch")(self._h, _ptr(A), A.shape[0], a, b, c, data_type,
+                                                        ctypes.c_float(threshold), _ptr(m), nthreads)
         return m
 
     def ndft_forward(self, img: np.ndarray) -> np.ndarray:
