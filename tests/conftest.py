@@ -37,6 +37,12 @@ def min_abs_tilt_index(tilts):
     return idx
 
 
+def cfg2_fp64(z):
+    """The FP64 oracle's result stored in tests/golden/cfg2.npz (as its
+    int16-quantised difference from the reference's), in float64."""
+    return z["ref_m"].astype(np.float64) + z["fp64_minus_ref_q"].astype(np.float64) * float(z["fp64_minus_ref_step"])
+
+
 @pytest.fixture(scope="session")
 def golden():
     return {n: load_golden(n) for n in ("a", "b", "c", "cli")}

@@ -14,7 +14,10 @@ full production schedule (-iter 10,280,10, data type 2, threshold 0):
   phase "oracle" (any machine; about 4 minutes on 8 cores):
       python tests/golden/make_golden_cfg2.py --phase oracle --ref DIR/cfg2_ref.npz
     adds the FP64 oracle's solve of the same rows for the same iteration
-    count (m_fp64, stored as float32) and writes tests/golden/cfg2.npz.
+    count and writes tests/golden/cfg2.npz.  The FP64 result is stored as its
+    difference from the reference's, quantised to int16 (fp64_minus_ref_q,
+    step fp64_minus_ref_step): m_fp64 = ref_m + q * step, exact to ~5e-11 of
+    the image's largest value (m_fp64() below rebuilds it).
 
 The rows are stored, so the tests never regenerate them.
 """
@@ -74,10 +77,20 @@ def phase_oracle(ref_path, out_path):
     z = dict(np.load(ref_path))
     p = OraclePlan(int(z["nx"]), int(z["thickness"]), z["tilts"], "f64")
     m64 = p.reconstruct(z["rows"], tuple(int(v) for v in z["sched"]), int(z["data_type"]), float(z["threshold"]))
-    z["m_fp64"] = m64.astype(np.float32)
+    d = m64 - z["ref_m"].astype(np.float64)
+    step = max(float(np.abs(d).max()), 1e-300) / 32000.0
+    z["fp64_minus_ref_q"] = np.round(d / step).astype(np.int16)
+    z["fp64_minus_ref_step"] = np.float64(step)
     np.savez_compressed(out_path, **z)
-    rel = [np.linalg.norm(z["m_fp64"][s] - z["ref_m"][s]) / np.linalg.norm(z["m_fp64"][s]) for s in range(len(m64))]
-    print(f"cfg2.npz written; reference vs FP64 oracle: max relative L2 {max(rel):.3e}")
+    back = m_fp64(z)
+    rel = [np.linalg.norm(m64[s] - z["ref_m"][s]) / np.linalg.norm(m64[s]) for s in range(len(m64))]
+    enc = float(np.abs(back - m64).max() / np.abs(m64).max())
+    print(f"cfg2.npz written; reference vs FP64 oracle: max relative L2 {max(rel):.3e}; encoding error {enc:.1e}")
+
+
+def m_fp64(z):
+    """The FP64 oracle's result (float64) from a loaded cfg2.npz."""
+    return z["ref_m"].astype(np.float64) + z["fp64_minus_ref_q"].astype(np.float64) * float(z["fp64_minus_ref_step"])
 
 
 def main():

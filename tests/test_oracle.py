@@ -183,3 +183,13 @@ def test_icon_weights_match_oracle_weights():
         t = np.asarray(tilts, np.float32)
         _, w_o, _ = OraclePlan(nx, 16, t, "f64").geometry()
         assert np.array_equal(weights(nx, t).ravel(), w_o)
+
+
+def test_reference_and_fp64_oracle_agree_at_production_size():
+    # The cfg2 fixture: the reference's 300-iteration result on 16 slices of
+    # the 1024x300, 61-tilt workload and the FP64 oracle's on the same rows.
+    from conftest import cfg2_fp64
+    z = load_golden("cfg2")
+    m64 = cfg2_fp64(z)
+    for s in range(int(z["S"])):
+        assert rel_l2(z["ref_m"][s], m64[s]) < 1e-5
