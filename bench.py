@@ -284,10 +284,11 @@ def reference_gpu_leg(tilts, rows_dev, plan, nslices=64):
     return res
 
 
-def parity_leg(plan_factory):
+def parity_leg(plan_factory, operator):
     """This build's reconstruction of the 16 slices of tests/golden/cfg2.npz
-    (seeded random slices of the workload, full schedule) against the
-    reference's result (ref_harness) and the FP64 oracle's, same iterations."""
+    (seeded random slices of the workload, full schedule) with the given
+    normal operator, against the reference's result (ref_harness) and the
+    FP64 oracle's, same iterations."""
     import torch
     from feilab_b200.train_warmstart import frc_mean
     path = os.path.join(ROOT, "tests", "golden", "cfg2.npz")
@@ -296,11 +297,13 @@ def parity_leg(plan_factory):
     z = np.load(path)
     S = int(z["S"])
     plan = plan_factory(S)
+    plan.set_operator(operator)
     rows = torch.from_numpy(np.ascontiguousarray(z["rows"])).cuda()
     m = plan.solve(plan.prepare_rhs(rows), tuple(int(v) for v in z["sched"]), int(z["data_type"]),
                    float(z["threshold"])).cpu()
     plan.close()
-    m64 = torch.from_numpy(z["m_fp64"].astype(np.float32))
+    m64 = torch.from_numpy(z["ref_m"].astype(np.float64) +
+                           z["fp64_minus_ref_q"].astype(np.float64) * float(z["fp64_minus_ref_step"]))
     mref = torch.from_numpy(z["ref_m"].astype(np.float32))
 
     def rel(a, b):
@@ -345,66 +348,84 @@ def run_ours(args):
     def max_over_ranks(x):
         return sharding.max_over_ranks(x, world, device=dev)
 
-    # ---- device-resident inputs (value) -------------------------------------
-    for i in range(args.warmup):
-        A = plan.prepare_rhs(rows[i])
-        plan.solve(A, SCHED, DATA_TYPE, THRESHOLD)
-    barrier()
     uuid = None
     try:
         uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     except Exception:
         pass
-    plan.trace(True)
-    plan.trace_read()
-    launches0 = plan.launch_count()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(uuid) as clk:
-        barrier()
-        ev0.record(stream)
-        for i in range(args.warmup, nsteps):
-            A = plan.prepare_rhs(rows[i])
-            m = plan.solve(A, SCHED, DATA_TYPE, THRESHOLD)
-        ev1.record(stream)
-        barrier()
-    launches = plan.launch_count() - launches0
-    trace = plan.trace_read()
-    plan.trace(False)
-    t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
-    clocks = clk.summary()
-    value = sharding.job_rate(world, S, args.steps, t_dev)
 
-    # ---- end to end: host rows in, host slices out ------------------------
+    def timed_device(op):
+        """Device-resident rows in, K timed steps (input stage + schedule),
+        CUDA events on the launch stream, max over ranks."""
+        plan.set_operator(op)
+        for i in range(args.warmup):
+            plan.solve(plan.prepare_rhs(rows[i]), SCHED, DATA_TYPE, THRESHOLD)
+        barrier()
+        plan.trace(True)
+        plan.trace_read()
+        launches0 = plan.launch_count()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(uuid) as clk:
+            barrier()
+            ev0.record(stream)
+            for i in range(args.warmup, nsteps):
+                plan.solve(plan.prepare_rhs(rows[i]), SCHED, DATA_TYPE, THRESHOLD)
+            ev1.record(stream)
+            barrier()
+        launches = plan.launch_count() - launches0
+        trace = plan.trace_read()
+        plan.trace(False)
+        t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+        return {"value": sharding.job_rate(world, S, args.steps, t), "t": t, "trace": trace, "launches": launches,
+                "clocks": clk.summary()}
+
     h_rows = torch.empty((nsteps, S, len(tilts), NX), dtype=torch.float32, pin_memory=True)
     h_rows.copy_(rows.cpu())
     h_out = torch.empty((S, NX, THICK), dtype=torch.float32, pin_memory=True)
-    for i in range(args.warmup):
-        plan.reconstruct_host(h_rows[i], SCHED, DATA_TYPE, THRESHOLD, out=h_out, stream=stream.cuda_stream)
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for i in range(args.warmup, nsteps):
-        plan.reconstruct_host(h_rows[i], SCHED, DATA_TYPE, THRESHOLD, out=h_out, stream=stream.cuda_stream)
-    e1.record(stream)
-    barrier()
-    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-    e2e = sharding.job_rate(world, S, args.steps, t_e2e)
 
-    # ---- roofline of the dominant kernel ----------------------------------
+    def timed_e2e(op):
+        """The same through icon_reconstruct_host: pinned host rows in, host
+        slices out, the copies inside the timed region."""
+        plan.set_operator(op)
+        for i in range(args.warmup):
+            plan.reconstruct_host(h_rows[i], SCHED, DATA_TYPE, THRESHOLD, out=h_out, stream=stream.cuda_stream)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.warmup, nsteps):
+            plan.reconstruct_host(h_rows[i], SCHED, DATA_TYPE, THRESHOLD, out=h_out, stream=stream.cuda_stream)
+        e1.record(stream)
+        barrier()
+        return sharding.job_rate(world, S, args.steps, max_over_ranks(e0.elapsed_time(e1) / 1e3))
+
+    slots = plan.B * ((S + plan.B - 1) // plan.B)
+
+    def kernel_table(trace):
+        total_ms = sum(v[1] for v in trace.values())
+        return {k: {"launches": v[0], "ms": round(v[1], 3), "share": round(v[1] / total_ms, 4),
+                    "gbs": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] > 0 and v[2] > 0 else None}
+                for k, v in trace.items() if v[0] > 0}
+
     peak, peak_kind = measured_peaks()
+    ops = [args.operator] + [o for o in ("nufft", "toeplitz") if o != args.operator]
+    runs = {}
+    for op in ops:
+        runs[op] = timed_device(op)
+        runs[op]["e2e"] = timed_e2e(op)
+    head = runs[args.operator]
+    value, t_dev, trace, e2e = head["value"], head["t"], head["trace"], head["e2e"]
+
+    # ---- roofline of the headline operator's dominant kernel ---------------
     dom = max((k for k in trace if trace[k][0] > 0), key=lambda k: trace[k][1])
     cnt, ms, by = trace[dom]
     achieved = (by / cnt) / (ms / cnt / 1e3) / 1e9
-    slots = plan.B * ((S + plan.B - 1) // plan.B)
     traffic_slot = dram_traffic_from_profile(dom)
-    total_ms = sum(v[1] for v in trace.values())
-    kernels = {k: {"launches": v[0], "ms": round(v[1], 3), "share": round(v[1] / total_ms, 4),
-                   "gbs": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] > 0 and v[2] > 0 else None}
-               for k, v in trace.items() if v[0] > 0}
     # NUFFT pair (forward R2C + adjoint) per slice-iteration: the model bytes
-    # of the reference's staged NUFFT over the time of our fused kernels.
-    fwd_ms = (trace["xpass_fwd"][1] + trace["ypass_fwd"][1] + trace["interp_fin"][1]) / 2.0
-    adj_ms = trace["ypass_adj"][1] + trace["xpass_adj"][1]
+    # of the reference's staged NUFFT over the time of our fused kernels, from
+    # the run with the NUFFT operator.
+    tn = runs["nufft"]["trace"]
+    fwd_ms = (tn["xpass_fwd"][1] + tn["ypass_fwd"][1] + tn["interp_fin"][1]) / 2.0
+    adj_ms = tn["ypass_adj"][1] + tn["xpass_adj"][1]
     slice_iters = slots * args.steps * sum(SCHED)
     pair_s = (fwd_ms + adj_ms) / 1e3 / slice_iters
     pair_gbs = PAIR_MODEL_BYTES / pair_s / 1e9
@@ -414,6 +435,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "slices_per_step": S, "iterations": sum(SCHED), "nx": NX, "thickness": THICK,
                        "tilts": len(tilts), "slices_per_group": plan.B, "parallelism": f"slices sharded over {world} GPU(s)",
+                       "operator": args.operator,
                        "l2": "inputs larger than L2 (per-step working set ~20 GB), no flush needed",
                        "stop": "fixed iteration count (the reference has no residual test)"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -422,14 +444,18 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": by / cnt},
             "nufft_pair": {"model_bytes_per_slice": PAIR_MODEL_BYTES, "gbs": round(pair_gbs, 1),
                            "frac": round(pair_gbs / peak, 4), "us_per_slice": round(pair_s * 1e6, 3)},
-            "kernels": kernels,
+            "kernels": kernel_table(trace),
             "e2e": {"value": e2e, "unit": "slices/s", "h2d_bytes_per_step": int(S * len(tilts) * NX * 4),
                     "d2h_bytes_per_step": int(S * NX * THICK * 4)},
-            "gpu_launches": int(launches),
-            "clocks": clocks}
+            "gpu_launches": int(head["launches"]),
+            "clocks": head["clocks"],
+            "operators": {op: {"value": r["value"], "e2e": r["e2e"], "ms_per_step": r["t"] / args.steps * 1e3,
+                               "kernels": kernel_table(r["trace"]), "clocks": r["clocks"]} for op, r in runs.items()}}
+    plan.set_operator(args.operator)
     line["warm_start"] = warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S)
     if rank == 0:
-        line["parity"] = parity_leg(lambda n: icon.IconPlan(NX, THICK, tilts, capacity=n, device=local))
+        line["parity"] = {op: parity_leg(lambda n: icon.IconPlan(NX, THICK, tilts, capacity=n, device=local), op)
+                          for op in ops}
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_leg(tilts, rows[0], plan)
         if "value" in line["reference_gpu"]:
@@ -507,6 +533,7 @@ def run_profile_case(args):
     S = 16
     rows, tilts = make_rows(list(range(S)), "cuda")
     plan = icon.IconPlan(NX, THICK, tilts, capacity=S)
+    plan.set_operator(args.operator)
     plan.trace(True)
     A = plan.prepare_rhs(rows)
     plan.solve(A, (0, 2, 0), DATA_TYPE, THRESHOLD)
@@ -525,6 +552,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference ICON-GPU leg")
+    ap.add_argument("--operator", default="nufft", choices=["nufft", "toeplitz"],
+                    help="normal operator of the headline run (the other is timed beside it)")
     ap.add_argument("--profile", action="store_true", help="run the small ncu case only")
     args = ap.parse_args()
     if args.profile:

@@ -187,10 +187,20 @@ struct icon_plan {
     // scratch sized for Gcap groups
     float2 *G1 = nullptr, *P = nullptr, *f = nullptr, *rhat = nullptr, *Ahwb = nullptr, *imgc = nullptr;
     float *m = nullptr, *rows = nullptr, *outrp = nullptr, *mout = nullptr;
+    float *nodes_xy = nullptr;   // [M][2] node coordinates on the device (Toeplitz kernel)
     double *part_rtr = nullptr, *part_rtar = nullptr, *alpha = nullptr;
     double *step_part = nullptr, *step = nullptr;   // relative update size (icon_solve_until)
     float *wgroup = nullptr;   // [Gcap][M] per-group weights while wgroups > 0
     int wgroups = 0;
+    // Normal operator of the iterations: ICON_OPERATOR_NUFFT (the reference's
+    // NUFFT pair) or ICON_OPERATOR_TOEPLITZ (A^H W A as a convolution with Kt).
+    int op = ICON_OPERATOR_NUFFT;
+    float *Kt = nullptr;        // [Gcap][n0][n1] Toeplitz kernels (one used unless per-group weights)
+    int kt_groups = 0;          // kernels computed for: 1 = the plan's weights, Gcap = per-group weights
+    bool kt_stale = true;
+    float *ones0 = nullptr, *ones1 = nullptr;   // unit deapodisation of the Toeplitz x-passes
+    size_t smem_yt = 0;
+    int na_rtar = 0;            // partial sums per group of the step length's denominator
     int k3_blocks = 0;
     // reprojection lines, keyed by the .tlt angle
     std::map<float, std::unique_ptr<NodeTables>> lines;
@@ -241,6 +251,17 @@ struct icon_plan {
         g.cx = cx; g.cy = cy; g.rcx = rcx; g.rcy = rcy; g.row_off = t.row_off; g.ent_jt = t.ent_jt; g.ent_iy0 = t.ent_iy0;
         g.ent_lb = t.ent_lb; g.ent_phiy = t.ent_phiy; g.ent_pxy = t.ent_pxy;
         g.tw0 = tw0; g.tw0h = tw0h; g.tw1 = tw1;
+        g.Kt = Kt;
+        g.kstride = kt_groups > 1 ? (size_t)n0 * n1 : 0;
+        return g;
+    }
+    // The Toeplitz iteration's view: the plan's nodes with unit deapodisation
+    // (its x-passes only pad and crop).
+    Geo geo_unit() const
+    {
+        Geo g = geo(nodes);
+        g.rcx = ones0;
+        g.rcy = ones1;
         return g;
     }
     Geo1 geo1() const
@@ -254,7 +275,7 @@ struct icon_plan {
 
 namespace {
 
-enum Kind { K_XF = 0, K_YF, K_FIN, K_YA, K_XA, K_ALPHA, K_UPD, K_ROWS, K_LAYOUT, K_ROWADJ };
+enum Kind { K_XF = 0, K_YF, K_FIN, K_YA, K_XA, K_ALPHA, K_UPD, K_ROWS, K_LAYOUT, K_ROWADJ, K_YT, K_YQ };
 
 // Launches one kernel; counts it and, while tracing, brackets it by events
 // and records its algorithmic bytes (compulsory reads + writes, see
@@ -479,10 +500,15 @@ icon_status launch_rows(icon_plan *p, const float *d_rows, int S, int G, float2 
     return launch_rows_at(p, d_rows, (size_t)p->nz * p->nx, (size_t)p->nx, INT_MAX, S, G, bout, st);
 }
 
+icon_status launch_iteration_toep(icon_plan *p, int G, bool clamp, int data_type, float thr, double *hist_a,
+                                  double *hist_r, cudaStream_t st, bool measure_step);
+
 // One ICON iteration over G groups (Iteration2.cu:53-132 with Alpha2).
 icon_status launch_iteration(icon_plan *p, int G, bool clamp, int data_type, float thr, double *hist_a, double *hist_r,
                              cudaStream_t st, bool measure_step = false)
 {
+    if (p->op == ICON_OPERATOR_TOEPLITZ)
+        return launch_iteration_toep(p, G, clamp, data_type, thr, hist_a, hist_r, st, measure_step);
     ICON_TRY(launch_forward(p, p->nodes, p->m, true, G, 1, p->f, st));          // f = W A m
     ICON_TRY(launch_adjoint(p, p->f, G, 1, p->rhat, st));                       // rhat = A^H f - Ahwb, ||rhat||^2
     ICON_TRY(launch_forward(p, p->nodes, p->rhat, false, G, 2, nullptr, st));   // r = A rhat, sum w|r|^2
@@ -501,11 +527,66 @@ icon_status launch_iteration(icon_plan *p, int G, bool clamp, int data_type, flo
     return ICON_OK;
 }
 
+// The Toeplitz kernels of the plan's weights (one) or, with per-group
+// weights, of every group's (icon_plan_set_group_weights), when stale.
+icon_status ensure_toeplitz(icon_plan *p, cudaStream_t st)
+{
+    if (p->op != ICON_OPERATOR_TOEPLITZ || !p->kt_stale) return ICON_OK;
+    const int groups_needed = p->wgroups > 0 ? p->Gcap : 1;
+    if (!p->Kt) ICON_TRY(p->arena.alloc(&p->Kt, (size_t)p->Gcap * p->n0 * p->n1));
+    float *xy_d = nullptr;
+    if (!p->nodes_xy) ICON_TRY(p->arena.upload(&p->nodes_xy, p->xy.data(), p->xy.size()));
+    xy_d = p->nodes_xy;
+    const float *w = p->wgroups > 0 ? p->wgroup : p->nodes.w;
+    dim3 grid((p->n1 + icon::kToepTile - 1) / icon::kToepTile, (p->n0 + icon::kToepTile - 1) / icon::kToepTile,
+              groups_needed);
+    icon::k_toep_kernel<<<grid, 256, 0, st>>>(xy_d, w, p->wgroups > 0 ? (size_t)p->M : 0, p->M, p->N0, p->N1, p->n0,
+                                              p->n1, p->Kt);
+    ICON_CUDA(cudaGetLastError());
+    p->kt_groups = groups_needed;
+    p->kt_stale = false;
+    return ICON_OK;
+}
+
+// One ICON iteration with A^H W A as a convolution (k_ypass_toep): the same
+// steps as launch_iteration, f-hat = A^H W A m and rtar = r^H A^H W A r
+// taken from the Toeplitz form instead of the NUFFT pair.
+icon_status launch_iteration_toep(icon_plan *p, int G, bool clamp, int data_type, float thr, double *hist_a,
+                                  double *hist_r, cudaStream_t st, bool measure_step)
+{
+    Geo g = p->geo_unit();
+    const double slots = (double)G * p->B;
+    const double NN = (double)p->N0 * p->N1, G1b = (double)p->n0 * p->N1 * 8, Kb = (double)p->n0 * p->n1 * 4;
+    dim3 gx(p->N1, G), gy(G, p->n0);
+    WITH_B(p->B,
+        LAUNCH_B(p, K_XF, st, (NN * 4 + G1b) * slots, L::xpass_fwd_full(p->ex, gx, p->thr_x, p->smem_x, st, g, p->m, p->G1));
+        LAUNCH_B(p, K_YT, st, (2 * G1b) * slots + Kb * G, L::ypass_toep(p->ey, gy, p->thr_y, p->smem_yt, st, g, p->G1));
+        LAUNCH_B(p, K_XA, st, (G1b + NN * 16) * slots,
+                 L::xpass_adj(1, p->ex, gx, p->thr_x, p->smem_x + sizeof(double) * p->thr_x, st, g, p->G1, p->rhat,
+                              p->Ahwb, p->part_rtr));
+        LAUNCH_B(p, K_XF, st, (NN * 8 + G1b) * slots, L::xpass_fwd(false, p->ex, gx, p->thr_x, p->smem_x, st, g, p->rhat, p->G1));
+        LAUNCH_B(p, K_YQ, st, G1b * slots + Kb * G,
+                 L::ypass_toep_quad(p->ey, gy, p->thr_y, p->smem_yt, st, g, p->G1, p->part_rtar)))
+    LAUNCH(p, K_ALPHA, st, icon::k_alpha<<<G, 32 * p->B, 0, st>>>(p->part_rtr, p->N1, p->part_rtar, p->n0, p->B, p->alpha, hist_a, hist_r));
+    int per_group = p->N1 * p->N0 * p->B;
+    dim3 gu((unsigned)std::min<size_t>(((size_t)per_group + 255) / 256, 512), G);
+    WITH_B(p->B, LAUNCH_B(p, K_UPD, st, stage_bytes(p, p->nodes).upd * G * p->B,
+                          L::update(gu, st, p->m, p->rhat, p->alpha, per_group, clamp ? 1 : 0, data_type, thr,
+                                    measure_step ? p->step_part : nullptr)))
+    if (measure_step) {
+        const int slots_i = G * p->B;
+        LAUNCH(p, K_UPD, st, icon::k_step_reduce<<<(slots_i + 127) / 128, 128, 0, st>>>(p->step_part, (int)gu.x, p->B, slots_i, p->step));
+    }
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
 // After the row transform of G groups: Ahwb = A^H W b, m = 0, the schedule's
 // iterations (MainCode.cu:115-140 with Iteration3).
 icon_status solve_from_rows(icon_plan *p, const icon_solve_cfg *cfg, int G, cudaStream_t st)
 {
     const int a = cfg->infr_before, b = cfg->icon, c = cfg->infr_after, iters = a + b + c;
+    ICON_TRY(ensure_toeplitz(p, st));
     ICON_TRY(launch_adjoint(p, p->f, G, 0, p->Ahwb, st));
     size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
     ICON_CUDA(cudaMemsetAsync(p->m, 0, tot * sizeof(float), st));
@@ -666,14 +747,15 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
     p->smem_x = (size_t)p->n0 * B * sizeof(float2);
     p->smem_y = icon::ypass_fwd_smem(p->n1, B);
     p->smem_ya = icon::ypass_adj_smem(p->n1, B);
+    p->smem_yt = icon::ypass_toep_smem(p->n1, B);
     int smem_max = 0;
     ICON_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     size_t need_x = p->smem_x + sizeof(double) * p->thr_x;
-    if ((size_t)smem_max < std::max(need_x, std::max(p->smem_y, p->smem_ya)))
+    if ((size_t)smem_max < std::max(std::max(need_x, p->smem_yt), std::max(p->smem_y, p->smem_ya)))
         return fail(ICON_ERR_INVALID, "FFT buffer exceeds shared memory");
     {
         cudaError_t e = cudaSuccess;
-        WITH_B(B, e = L::set_smem(p->ex, p->ey, p->smem_x, need_x, p->smem_y, p->smem_ya))
+        WITH_B(B, e = L::set_smem(p->ex, p->ey, p->smem_x, need_x, p->smem_y, p->smem_ya, p->smem_yt))
         if (e != cudaSuccess) return fail(ICON_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     }
     // Scratch for Gcap groups.
@@ -692,7 +774,13 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
     ICON_TRY(p->arena.alloc(&p->mout, (size_t)p->cap * NN));
     p->k3_blocks = (p->M * B + 255) / 256;
     ICON_TRY(p->arena.alloc(&p->part_rtr, G * p->N1 * Bz));
-    ICON_TRY(p->arena.alloc(&p->part_rtar, G * p->k3_blocks * Bz));
+    // rtar partials: one per k_interp_fin block (NUFFT), one per grid row (Toeplitz)
+    ICON_TRY(p->arena.alloc(&p->part_rtar, G * std::max(p->k3_blocks, p->n0) * Bz));
+    {
+        std::vector<float> one((size_t)std::max(p->N0, p->N1), 1.0f);
+        ICON_TRY(p->arena.upload(&p->ones0, one.data(), (size_t)p->N0));
+        ICON_TRY(p->arena.upload(&p->ones1, one.data(), (size_t)p->N1));
+    }
     ICON_TRY(p->arena.alloc(&p->alpha, G * Bz));
     ICON_TRY(p->arena.alloc(&p->step_part, G * 512 * Bz * 2));
     ICON_TRY(p->arena.alloc(&p->step, G * Bz));
@@ -749,6 +837,7 @@ icon_status icon_plan_set_group_weights(icon_plan *p, const float *h_w, int ngro
 {
     if (!p) return fail(ICON_ERR_INVALID, "null plan");
     if (ngroups == 0) {
+        if (p->wgroups != 0) p->kt_stale = true;
         p->wgroups = 0;
         return ICON_OK;
     }
@@ -761,6 +850,16 @@ icon_status icon_plan_set_group_weights(icon_plan *p, const float *h_w, int ngro
     for (int gi = ngroups; gi < p->Gcap; ++gi)   // the remaining groups keep the plan's own weights
         ICON_CUDA(cudaMemcpy(p->wgroup + gi * M, p->nodes.w, sizeof(float) * M, cudaMemcpyDeviceToDevice));
     p->wgroups = ngroups;
+    p->kt_stale = true;
+    return ICON_OK;
+}
+
+icon_status icon_plan_set_operator(icon_plan *p, int op)
+{
+    if (!p) return fail(ICON_ERR_INVALID, "null plan");
+    if (op != ICON_OPERATOR_NUFFT && op != ICON_OPERATOR_TOEPLITZ) return fail(ICON_ERR_INVALID, "unknown operator");
+    if (op != p->op) p->kt_stale = true;
+    p->op = op;
     return ICON_OK;
 }
 
@@ -1012,6 +1111,7 @@ icon_status icon_solve(icon_plan *p, const icon_solve_cfg *cfg, const void *d_Ah
     cudaStream_t st = (cudaStream_t)stream;
     int G = groups(p, S);
     size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
+    ICON_TRY(ensure_toeplitz(p, st));
     LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float2><<<grid1d(tot), 256, 0, st>>>((const float2 *)d_Ahwb, p->Ahwb, S, p->N0, p->N1, p->B, tot));
     if (warm_start) LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float><<<grid1d(tot), 256, 0, st>>>(d_m, p->m, S, p->N0, p->N1, p->B, tot));
     else ICON_CUDA(cudaMemsetAsync(p->m, 0, tot * sizeof(float), st));
@@ -1059,6 +1159,7 @@ icon_status icon_solve_until(icon_plan *p, const icon_solve_cfg *cfg, const void
     cudaStream_t st = (cudaStream_t)stream;
     const int G = groups(p, S);
     const size_t tot = (size_t)G * p->N1 * p->N0 * p->B, slots = (size_t)G * p->B;
+    ICON_TRY(ensure_toeplitz(p, st));
     LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float2><<<grid1d(tot), 256, 0, st>>>((const float2 *)d_Ahwb, p->Ahwb, S, p->N0, p->N1, p->B, tot));
     if (warm_start) LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float><<<grid1d(tot), 256, 0, st>>>(d_m, p->m, S, p->N0, p->N1, p->B, tot));
     else ICON_CUDA(cudaMemsetAsync(p->m, 0, tot * sizeof(float), st));

@@ -29,6 +29,34 @@ void Launch<B>::xpass_fwd(bool real_in, int E, dim3 grid, int threads, size_t sm
 }
 
 template <int B>
+void Launch<B>::xpass_fwd_full(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
+                               const float *in, float2 *G1)
+{
+    if (g.n0 / 2 >= E) {   // half-length FFT per slice, as xpass_fwd
+        if (E == 32) k_xpass_fwd_r2c<B, 32, true><<<grid, threads / 2, smem / 2, st>>>(g, in, G1);
+        else k_xpass_fwd_r2c<B, 16, true><<<grid, threads / 2, smem / 2, st>>>(g, in, G1);
+        return;
+    }
+    if (E == 32) k_xpass_fwd<true, B, 32, true><<<grid, threads, smem, st>>>(g, in, G1);
+    else k_xpass_fwd<true, B, 16, true><<<grid, threads, smem, st>>>(g, in, G1);
+}
+
+template <int B>
+void Launch<B>::ypass_toep(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, float2 *G1)
+{
+    if (E == 32) k_ypass_toep<B, 32><<<grid, threads, smem, st>>>(g, G1);
+    else k_ypass_toep<B, 16><<<grid, threads, smem, st>>>(g, G1);
+}
+
+template <int B>
+void Launch<B>::ypass_toep_quad(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
+                                const float2 *G1, double *part)
+{
+    if (E == 32) k_ypass_toep_quad<B, 32><<<grid, threads, smem, st>>>(g, G1, part);
+    else k_ypass_toep_quad<B, 16><<<grid, threads, smem, st>>>(g, G1, part);
+}
+
+template <int B>
 void Launch<B>::ypass_fwd(int E, bool herm, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
                           const float2 *G1, float2 *P)
 {
@@ -106,7 +134,8 @@ void Launch<B>::update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat,
 }
 
 template <int B>
-cudaError_t Launch<B>::set_smem(int ex, int ey, size_t smem_x, size_t need_x, size_t smem_y, size_t smem_ya)
+cudaError_t Launch<B>::set_smem(int ex, int ey, size_t smem_x, size_t need_x, size_t smem_y, size_t smem_ya,
+                                size_t smem_yt)
 {
     cudaError_t e = cudaSuccess;
     auto set = [&](const void *fn, size_t bytes) {
@@ -117,6 +146,8 @@ cudaError_t Launch<B>::set_smem(int ex, int ey, size_t smem_x, size_t need_x, si
         set((const void *)k_xpass_fwd<true, B, 32>, smem_x);
         set((const void *)k_xpass_fwd<false, B, 32>, smem_x);
         set((const void *)k_xpass_fwd_r2c<B, 32>, smem_x / 2);
+        set((const void *)k_xpass_fwd_r2c<B, 32, true>, smem_x / 2);
+        set((const void *)k_xpass_fwd<true, B, 32, true>, smem_x);
         set((const void *)k_xpass_adj<0, B, 32>, need_x);
         set((const void *)k_xpass_adj<1, B, 32>, need_x);
         set((const void *)k_rows_fwd<B, 32>, smem_x);
@@ -125,6 +156,8 @@ cudaError_t Launch<B>::set_smem(int ex, int ey, size_t smem_x, size_t need_x, si
         set((const void *)k_xpass_fwd<true, B, 16>, smem_x);
         set((const void *)k_xpass_fwd<false, B, 16>, smem_x);
         set((const void *)k_xpass_fwd_r2c<B, 16>, smem_x / 2);
+        set((const void *)k_xpass_fwd_r2c<B, 16, true>, smem_x / 2);
+        set((const void *)k_xpass_fwd<true, B, 16, true>, smem_x);
         set((const void *)k_xpass_adj<0, B, 16>, need_x);
         set((const void *)k_xpass_adj<1, B, 16>, need_x);
         set((const void *)k_rows_fwd<B, 16>, smem_x);
@@ -134,11 +167,15 @@ cudaError_t Launch<B>::set_smem(int ex, int ey, size_t smem_x, size_t need_x, si
         set((const void *)k_ypass_fwd<B, 32, false>, smem_y);
         set((const void *)k_ypass_fwd<B, 32, true>, smem_y);
         set((const void *)k_ypass_adj<B, 32, false>, smem_ya);
+        set((const void *)k_ypass_toep<B, 32>, smem_yt);
+        set((const void *)k_ypass_toep_quad<B, 32>, smem_yt);
     } else {
         set((const void *)k_ypass_fwd<B, 16, false>, smem_y);
         set((const void *)k_ypass_fwd<B, 16, true>, smem_y);
         set((const void *)k_ypass_adj<B, 16, false>, smem_ya);
         set((const void *)k_ypass_adj<B, 16, true>, smem_ya);
+        set((const void *)k_ypass_toep<B, 16>, smem_yt);
+        set((const void *)k_ypass_toep_quad<B, 16>, smem_yt);
     }
     return e;
 }

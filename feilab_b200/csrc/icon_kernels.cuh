@@ -59,6 +59,8 @@ struct Geo {
     const float2 *tw0;     // [n0] exp(-2 pi i q / n0)
     const float2 *tw0h;    // [n0/2] exp(-2 pi i q / (n0/2))
     const float2 *tw1;     // [n1] exp(-2 pi i q / n1)
+    const float *Kt;       // [n0][n1] Toeplitz kernel of A^H W A, group g's at Kt + g*kstride
+    size_t kstride;        // 0: one kernel for every group; n0*n1: one per group
 };
 
 // 1-D row-transform tables (cunfft_initPlan_1d, NU:1298-1391).
@@ -151,7 +153,7 @@ __device__ __forceinline__ void store_b(float2 *__restrict__ p, const float2 (&v
 // a multiplication by the reciprocals, within 2 ulp of the reference's
 // quotient).  The first FFT pass reads the image column directly, the last
 // writes G1.
-template <bool REAL_IN, int B, int E>
+template <bool REAL_IN, int B, int E, bool FULL = false>
 __global__ void FFT_BOUNDS(E) k_xpass_fwd(Geo g, const void *__restrict__ in, float2 *__restrict__ G1)
 {
     extern __shared__ float2 s[];
@@ -180,9 +182,9 @@ __global__ void FFT_BOUNDS(E) k_xpass_fwd(Geo g, const void *__restrict__ in, fl
         return make_float2(v.x * r, v.y * r);
     };
     // A real image's rows n0/2+1.. are the conjugates of rows n0/2-1..1;
-    // the forward y-pass (HERM) reads rows 0..n0/2 only.
+    // the forward y-pass (HERM) reads rows 0..n0/2 only (FULL: all rows).
     auto st = [=](int x, int b, float2 v) {
-        if (!REAL_IN || x <= (n >> 1)) out[(size_t)x * N1 * B + b] = v;
+        if (!REAL_IN || FULL || x <= (n >> 1)) out[(size_t)x * N1 * B + b] = v;
     };
     fft_fused<B, B, E>(s, n, g.lg0, g.tw0, -1.f, ld, st);
 }
@@ -193,9 +195,10 @@ __global__ void FFT_BOUNDS(E) k_xpass_fwd(Geo g, const void *__restrict__ in, fl
 // length N per slice (blockDim = N*B/E), and with Z = FFT(z), W = exp(-2 pi i/n0):
 //   X(k) = (Z(k) + conj Z(N-k)) / 2 - i W^k (Z(k) - conj Z(N-k)) / 2,
 // indices of Z mod N, written for k = 0..n0/2 (the rows the Hermitian y-pass
-// reads).  Each slice stays its own transform, so results do not depend on
-// which slices share a group.
-template <int B, int E>
+// reads) and, with FULL, also for k = n0/2+1..n0-1 as the conjugates
+// X(n0 - k)* (the Toeplitz y-pass takes every row).  Each slice stays its own
+// transform, so results do not depend on which slices share a group.
+template <int B, int E, bool FULL = false>
 __global__ void FFT_BOUNDS(E) k_xpass_fwd_r2c(Geo g, const float *__restrict__ in, float2 *__restrict__ G1)
 {
     extern __shared__ float2 s[];
@@ -227,7 +230,9 @@ __global__ void FFT_BOUNDS(E) k_xpass_fwd_r2c(Geo g, const float *__restrict__ i
         const float2 fe = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
         const float2 fo = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
         const float2 w = __ldg(&g.tw0[k]);
-        out[(size_t)k * N1 * B + b] = cadd(fe, cmul(w, fo));
+        const float2 v = cadd(fe, cmul(w, fo));
+        out[(size_t)k * N1 * B + b] = v;
+        if (FULL && k > 0 && k < N) out[(size_t)(n - k) * N1 * B + b] = make_float2(v.x, -v.y);
     }
 }
 
@@ -1036,6 +1041,215 @@ __global__ void k_update(float *__restrict__ m, const float2 *__restrict__ rhat,
             o[1] = s1;
         }
     }
+}
+
+// ------------------------------------------------------------ Toeplitz ----
+// The normal operator of the iteration, A^H W A, as a two-dimensional
+// convolution.  For the exact transform, (A^H W A m)[X] = sum_X' m[X'] t[X - X']
+// with t[d] = sum_j w_j exp(+2 pi i x_j . d) for |d_k| < N_k: a Toeplitz
+// matrix.  On the n0 x n1 grid (n_k >= 2 N_k, so the circular convolution of
+// the zero-padded image with t is the linear one on the image), with
+// unnormalised FFTs F (e^{-2 pi i}) and F^-1 (e^{+2 pi i}):
+//   A^H W A m = crop F^-1( K . F(pad m) ),
+//   K[k0][k1] = F(t)[k] / (n0 n1)
+//             = 1/(n0 n1) sum_j w_j D_N0(x_j0 - k0/n0) D_N1(x_j1 - k1/n1),
+// with the Dirichlet kernel D_N(u) = sum_{|d|<N} e^{2 pi i u d}
+//                                  = sin(pi u (2N-1)) / sin(pi u)   (2N-1 at integer u).
+// K is real.  The step length's denominator sum_j w_j |(A r)_j|^2 is the
+// quadratic form r^H A^H W A r = sum_k K[k] |F(pad r)[k]|^2.  The reference
+// evaluates both with its Gaussian-window NUFFTs (Iteration2.cu:53-96,
+// alpha_new2.cu:26-114); this is the same operator without the window's
+// approximation (they differ by the window error, ~1e-6 relative).
+//
+// K is a sum over the M nodes of rank-one products, computed in double as a
+// matrix product: a CTA owns a 64 x 64 tile of K (thread: 4 x 4 entries),
+// takes the nodes 32 at a time, evaluates their Dirichlet factors for the
+// tile's 64 k0 and 64 k1 into shared memory, and accumulates.  sin(pi u) and
+// sin(pi u (2N-1)) at u = x - k/n are formed from per-node and per-k sines
+// and cosines by the angle-difference formula; every argument is exact in
+// double (x is a float, k/n a dyadic fraction).
+constexpr int kToepTile = 64;
+constexpr int kToepNodes = 32;
+
+// u = x - k/n is exact in double; at an integer u the angle-difference
+// formula leaves rounding noise in both sines, so integers are caught first.
+__device__ __forceinline__ double dirichlet(double x, double kn, double sa, double ca, double sb, double cb,
+                                            double sk, double ck, double skb, double ckb, double twoNm1)
+{
+    const double u = x - kn;
+    if (u == rint(u)) return twoNm1;
+    const double den = sa * ck - ca * sk;           // sin(pi (x - k/n))
+    const double num = sb * ckb - cb * skb;         // sin(pi (2N-1) (x - k/n))
+    return num / den;
+}
+
+#ifndef ICON_KERNELS_TEMPLATES_ONLY
+// xy: [M][2] node coordinates, w: [M] weights (group g's at w + g*wstride for
+// blockIdx.z = g); K: [G][n0][n1] float.
+__global__ void __launch_bounds__(256) k_toep_kernel(const float *__restrict__ xy, const float *__restrict__ w,
+                                                     size_t wstride, int M, int N0, int N1, int n0, int n1,
+                                                     float *__restrict__ K)
+{
+    __shared__ __align__(16) double F0[kToepNodes][kToepTile];   // w_j D_N0(x_j0 - k0/n0)
+    __shared__ __align__(16) double F1[kToepNodes][kToepTile];   // D_N1(x_j1 - k1/n1)
+    __shared__ double nd[kToepNodes][10];            // per node: sin, cos of pi x0, pi (2N0-1) x0, same for x1; x0, x1
+    const int t = threadIdx.x;
+    const int k1b = blockIdx.x * kToepTile, k0b = blockIdx.y * kToepTile, grp = blockIdx.z;
+    const float *wg = w + (size_t)grp * wstride;
+    const double a0 = 2.0 * N0 - 1.0, a1 = 2.0 * N1 - 1.0;
+    // This thread's k for the factor tables: column c = t % 64 of both tiles,
+    // nodes t / 64 + 4 i.
+    const int c = t & (kToepTile - 1), r0 = t >> 6;
+    double sk0, ck0, skb0, ckb0, sk1, ck1, skb1, ckb1;
+    const double u0 = (double)(k0b + c) / n0, u1 = (double)(k1b + c) / n1;
+    {
+        sincospi(u0, &sk0, &ck0);
+        sincospi(a0 * u0, &skb0, &ckb0);
+        sincospi(u1, &sk1, &ck1);
+        sincospi(a1 * u1, &skb1, &ckb1);
+    }
+    const int ty = t >> 4, tx = t & 15;              // outputs k0 = 4 ty + i, k1 = 4 tx + j
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int j0 = 0; j0 < M; j0 += kToepNodes) {
+        __syncthreads();                             // the previous chunk's tables are consumed
+        if (t < kToepNodes) {
+            const int j = j0 + t;
+            double x0 = 0.0, x1 = 0.0;
+            if (j < M) {
+                x0 = (double)xy[2 * (size_t)j];
+                x1 = (double)xy[2 * (size_t)j + 1];
+            }
+            sincospi(x0, &nd[t][0], &nd[t][1]);
+            sincospi(a0 * x0, &nd[t][2], &nd[t][3]);
+            sincospi(x1, &nd[t][4], &nd[t][5]);
+            sincospi(a1 * x1, &nd[t][6], &nd[t][7]);
+            nd[t][8] = x0;
+            nd[t][9] = x1;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kToepNodes / 4; ++i) {
+            const int r = r0 + 4 * i, j = j0 + r;
+            const double wj = j < M ? (double)wg[j] : 0.0;
+            F0[r][c] = wj * dirichlet(nd[r][8], u0, nd[r][0], nd[r][1], nd[r][2], nd[r][3], sk0, ck0, skb0, ckb0, a0);
+            F1[r][c] = dirichlet(nd[r][9], u1, nd[r][4], nd[r][5], nd[r][6], nd[r][7], sk1, ck1, skb1, ckb1, a1);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int r = 0; r < kToepNodes; ++r) {
+            const double2 p0 = *reinterpret_cast<const double2 *>(&F0[r][4 * ty]);
+            const double2 p1 = *reinterpret_cast<const double2 *>(&F0[r][4 * ty + 2]);
+            const double2 q0 = *reinterpret_cast<const double2 *>(&F1[r][4 * tx]);
+            const double2 q1 = *reinterpret_cast<const double2 *>(&F1[r][4 * tx + 2]);
+            const double a[4] = {p0.x, p0.y, p1.x, p1.y}, b[4] = {q0.x, q0.y, q1.x, q1.y};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) acc[i][jj] = fma(a[i], b[jj], acc[i][jj]);
+        }
+    }
+    const double scale = 1.0 / ((double)n0 * (double)n1);
+    float *Kg = K + (size_t)grp * n0 * n1;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int k0 = k0b + 4 * ty + i;
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const int k1 = k1b + 4 * tx + jj;
+            if (k0 < n0 && k1 < n1) Kg[(size_t)k0 * n1 + k1] = (float)(acc[i][jj] * scale);
+        }
+    }
+}
+#endif  // ICON_KERNELS_TEMPLATES_ONLY
+
+// Shared memory of the Toeplitz y-passes: the row buffer [n1][SB], the
+// kernel's row [n1] float and the twiddle table (n1 <= 2048).
+__host__ __device__ inline size_t ypass_toep_smem(int n1, int B)
+{
+    size_t sb = (B == 8) ? 8 : (B == 4) ? 6 : B;
+    return (size_t)n1 * sb * sizeof(float2) + (size_t)n1 * sizeof(float) + ypass_tw_bytes(n1);
+}
+
+// Toeplitz y-pass: per (group, grid row x) the row of the x-transformed
+// padded image (the N1 values of G1 row x, placed at y = Y), FFT along y,
+// times K[x][.], inverse FFT along y, the N1 values y = Y < N1 written back to
+// row x of G1 (in place: a CTA reads its row whole before it writes).  One of
+// the two y-passes of A^H W A m; the x-passes are k_xpass_fwd_r2c<FULL> and
+// k_xpass_adj with unit deapodisation.
+template <int B, int E>
+__global__ void FFT_BOUNDS(E) k_ypass_toep(Geo g, float2 *__restrict__ G1)
+{
+    extern __shared__ float2 s[];
+    constexpr int SB = YfStride<B>::v;
+    constexpr bool kSwz = (B == 8);
+    const int grp = blockIdx.x, x = blockIdx.y, n = g.n1, N1 = g.N1;
+    float2 *buf = s;
+    float *krow = reinterpret_cast<float *>(s + (size_t)n * SB);
+    float2 *tw_s = reinterpret_cast<float2 *>(krow + n);
+    const float2 *tws = ypass_tw_shared(n) ? tw_s : g.tw1;
+    float2 *row = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
+    copy_async(buf, row, (size_t)N1 * B * sizeof(float2));        // [N1][B], contiguous
+    copy_async(krow, g.Kt + grp * g.kstride + (size_t)x * n, (size_t)n * sizeof(float));
+    if (ypass_tw_shared(n)) copy_async(tw_s, g.tw1, (size_t)n * sizeof(float2));
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    const float2 *in = buf;
+    auto ld = [=](int y, int b) -> float2 { return y < N1 ? in[y * B + b] : make_float2(0.f, 0.f); };
+    auto st2 = [=](int q, int b, float2 v) {
+        if (q < N1) row[(size_t)q * B + b] = v;
+    };
+    auto st = [=](int q, int b, float2 v) {
+        const float k = krow[q];
+        buf[q * SB + b] = make_float2(v.x * k, v.y * k);
+    };
+    fft_fused<B, SB, E, false, kSwz, true>(buf, n, g.lg1, tws, -1.f, ld, st);
+    __syncthreads();
+    auto ld2 = [=](int q, int b) -> float2 { return buf[q * SB + b]; };
+    fft_fused<B, SB, E, false, kSwz, true>(buf, n, g.lg1, tws, +1.f, ld2, st2);
+}
+
+// The quadratic form of the step length, sum_k K[k] |F(pad r)[k]|^2, for the
+// x-transformed r-hat in G1: per (group, row x) the FFT along y of the row
+// and the FP64 sum of K[x][k1] |.|^2 per slice into part[G][n0][B] (alpha1,
+// NU:1652-1661, in its Toeplitz form).  Nothing else is written.
+template <int B, int E>
+__global__ void FFT_BOUNDS(E) k_ypass_toep_quad(Geo g, const float2 *__restrict__ G1, double *__restrict__ part)
+{
+    extern __shared__ float2 s[];
+    constexpr int SB = YfStride<B>::v;
+    constexpr bool kSwz = (B == 8);
+    const int grp = blockIdx.x, x = blockIdx.y, n = g.n1, N1 = g.N1;
+    float2 *buf = s;
+    float *krow = reinterpret_cast<float *>(s + (size_t)n * SB);
+    float2 *tw_s = reinterpret_cast<float2 *>(krow + n);
+    const float2 *tws = ypass_tw_shared(n) ? tw_s : g.tw1;
+    const float2 *row = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
+    copy_async(buf, row, (size_t)N1 * B * sizeof(float2));
+    copy_async(krow, g.Kt + grp * g.kstride + (size_t)x * n, (size_t)n * sizeof(float));
+    if (ypass_tw_shared(n)) copy_async(tw_s, g.tw1, (size_t)n * sizeof(float2));
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    const float2 *in = buf;
+    auto ld = [=](int y, int b) -> float2 { return y < N1 ? in[y * B + b] : make_float2(0.f, 0.f); };
+    struct Quad {
+        const float *krow;
+        double acc;
+        __device__ __forceinline__ void operator()(int q, int, float2 v)
+        {
+            acc += (double)krow[q] * ((double)v.x * (double)v.x + (double)v.y * (double)v.y);
+        }
+    } st{krow, 0.0};
+    fft_fused<B, SB, E, false, kSwz, true>(buf, n, g.lg1, tws, -1.f, ld, st);
+    __syncthreads();
+    double *red = reinterpret_cast<double *>(buf);
+    const double r = block_sum_per_slice(st.acc, red, B);
+    if ((int)threadIdx.x < B) part[((size_t)grp * g.n0 + x) * B + threadIdx.x] = r;
 }
 
 }  // namespace icon

@@ -13,6 +13,15 @@ template <int B>
 struct Launch {
     static void xpass_fwd(bool real_in, int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
                           const void *in, float2 *G1);
+    // Forward x-pass of a real image with every row written (half-length FFT;
+    // rows past n0/2 as conjugates), for the Toeplitz y-pass.
+    static void xpass_fwd_full(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
+                               const float *in, float2 *G1);
+    // Toeplitz y-passes: A^H W A on the rows of G1 in place, and the step
+    // length's quadratic form into part[G][n0][B].
+    static void ypass_toep(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, float2 *G1);
+    static void ypass_toep_quad(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
+                                const float2 *G1, double *part);
     static void ypass_fwd(int E, bool herm, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, const float2 *G1,
                           float2 *P);
     static void interp_fin(int mode, dim3 grid, cudaStream_t st, const Geo &g, const float2 *P, float2 *f, double *part);
@@ -29,7 +38,8 @@ struct Launch {
     static void update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat, const double *alpha, int per_group,
                        int clamp, int data_type, float thr, double *step_part = nullptr);
     // Raises the dynamic shared-memory limit of every kernel variant a plan uses.
-    static cudaError_t set_smem(int ex, int ey, size_t smem_x, size_t need_x, size_t smem_y, size_t smem_ya);
+    static cudaError_t set_smem(int ex, int ey, size_t smem_x, size_t need_x, size_t smem_y, size_t smem_ya,
+                                size_t smem_yt);
 };
 
 }  // namespace icon

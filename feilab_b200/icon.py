@@ -56,6 +56,7 @@ def lib():
         L.icon_device_free.argtypes = [I, V]
         L.icon_weights.argtypes = [I, I, V, V]
         L.icon_plan_set_group_weights.argtypes = [P, V, I]
+        L.icon_plan_set_operator.argtypes = [P, I]
         L.icon_trace_enable.argtypes = [P, I]
         L.icon_trace_read.argtypes = [P, V, V, V]
         L.icon_launch_count.argtypes = [P]
@@ -66,7 +67,8 @@ def lib():
                      "icon_rows_forward", "icon_prepare_rhs", "icon_solve", "icon_solve_until", "icon_reproject",
                      "icon_reconstruct_host", "icon_trace_enable", "icon_trace_read", "icon_prepare_rhs_stack",
                      "icon_reconstruct_stack", "icon_reconstruct_stack_host", "icon_host_alloc", "icon_host_free",
-                     "icon_stack_upload", "icon_device_free", "icon_weights", "icon_plan_set_group_weights"):
+                     "icon_stack_upload", "icon_device_free", "icon_weights", "icon_plan_set_group_weights",
+                     "icon_plan_set_operator"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -142,6 +144,15 @@ class IconPlan:
             return
         w = np.ascontiguousarray(np.asarray(w, np.float32).reshape(-1, self.M))
         _check(lib().icon_plan_set_group_weights(self._h, w.ctypes.data_as(ctypes.c_void_p), w.shape[0]))
+
+    OPERATORS = {"nufft": 0, "toeplitz": 1}
+
+    def set_operator(self, op):
+        """Normal operator of the iterations: "nufft" (the reference's NUFFT
+        pair, default) or "toeplitz" (A^H W A as a convolution with the exact
+        kernel of the node set; see icon_plan_set_operator)."""
+        _check(lib().icon_plan_set_operator(self._h, self.OPERATORS[op]))
+        self.operator = op
 
     def geometry(self):
         xy = np.zeros((self.M, 2), np.float32)
@@ -330,16 +341,17 @@ class IconPlan:
                                                  int(S), int(outputs), cb, None, _stream()))
 
     TRACE_KINDS = ("xpass_fwd", "ypass_fwd", "interp_fin", "ypass_adj", "xpass_adj", "alpha", "update", "rows_fwd",
-                   "layout", "row_adj")
+                   "layout", "row_adj", "ypass_toep", "ypass_toep_quad")
 
     def trace(self, enable=True):
         _check(lib().icon_trace_enable(self._h, int(bool(enable))))
 
     def trace_read(self):
         """{kernel kind: (launches, total ms, algorithmic bytes)} since the last read."""
-        cnt = (ctypes.c_int * 10)()
-        ms = (ctypes.c_double * 10)()
-        by = (ctypes.c_double * 10)()
+        n = len(self.TRACE_KINDS)
+        cnt = (ctypes.c_int * n)()
+        ms = (ctypes.c_double * n)()
+        by = (ctypes.c_double * n)()
         _check(lib().icon_trace_read(self._h, ctypes.cast(cnt, ctypes.c_void_p), ctypes.cast(ms, ctypes.c_void_p),
                                      ctypes.cast(by, ctypes.c_void_p)))
         return {k: (int(cnt[i]), float(ms[i]), float(by[i])) for i, k in enumerate(self.TRACE_KINDS)}

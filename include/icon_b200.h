@@ -115,6 +115,24 @@ icon_status icon_weights(int nx, int ntilt, const float *tilt_deg, float *h_w);
  * one weight vector. */
 icon_status icon_plan_set_group_weights(icon_plan *plan, const float *h_w, int ngroups);
 
+/* Normal operator of the iterations of icon_solve, icon_solve_until and the
+ * reconstruct calls.  ICON_OPERATOR_NUFFT (the default) evaluates
+ * A^H W A m and the step length's w-weighted |A r|^2 with the Gaussian-window
+ * NUFFT pair, as Iteration3 does (Iteration2.cu:53-96, alpha_new2.cu:26-114).
+ * ICON_OPERATOR_TOEPLITZ uses that A^H W A is a Toeplitz operator: A^H W A m
+ * = crop F^-1(K . F(pad m)) on the n0 x n1 grid, and sum_j w_j |(A r)_j|^2 =
+ * sum_k K[k] |F(pad r)[k]|^2, with the real kernel
+ * K[k] = 1/(n0 n1) sum_j w_j D_N0(x_j0 - k0/n0) D_N1(x_j1 - k1/n1),
+ * D_N(u) = sin(pi u (2N-1)) / sin(pi u), computed on the device in double
+ * when first needed (and again after the weights change).  It is the exact
+ * operator of the node set, without the NUFFT window's approximation (the two
+ * differ by ~1e-6 relative per application), and needs no interpolation or
+ * gather.  The input stage (A^H W b) and reprojection use the NUFFT either
+ * way.  No counterpart in the reference. */
+#define ICON_OPERATOR_NUFFT 0
+#define ICON_OPERATOR_TOEPLITZ 1
+icon_status icon_plan_set_operator(icon_plan *plan, int op);
+
 /* Forward 2-D NUFFT of real images: d_nodes = A d_img.
  * Replaces cunfft_trafo_2d_R2C2 (NU:984-1076). */
 icon_status icon_nufft_forward(icon_plan *plan, const float *d_img, void *d_nodes, int S, void *stream);
@@ -238,8 +256,8 @@ icon_status icon_reconstruct_host(icon_plan *plan, const icon_solve_cfg *cfg, co
  * kinds returns the number of launches, their summed device time in ms and,
  * when h_bytes is not NULL, their summed algorithmic bytes (the data each
  * launch must read and write at least once), then clears the record.  Kinds, in order: xpass_fwd, ypass_fwd, interp_fin,
- * ypass_adj, xpass_adj, alpha, update, rows_fwd, layout, row_adj. */
-#define ICON_TRACE_KERNELS 10
+ * ypass_adj, xpass_adj, alpha, update, rows_fwd, layout, row_adj, ypass_toep, ypass_toep_quad. */
+#define ICON_TRACE_KERNELS 12
 icon_status icon_trace_enable(icon_plan *plan, int enable);
 icon_status icon_trace_read(icon_plan *plan, int *h_count, double *h_ms, double *h_bytes);
 

@@ -1,0 +1,150 @@
+"""The Toeplitz normal operator (icon_plan_set_operator(ICON_OPERATOR_TOEPLITZ)):
+A^H W A as a convolution with the exact kernel of the node set.
+
+Against the reference: whole solves on the golden fixtures must stay within
+the ICON-GPU parity bar (1e-4 relative L2 per slice; the Toeplitz operator
+and the reference's Gaussian-window NUFFT pair differ by the window's error,
+~1e-6 relative per application).  Against an exact computation: one
+iteration from a random start, with A and A^H the oracle's direct NDFT in
+FP64, must agree to float rounding (1e-5), which checks the kernel, the
+convolution and the step length's quadratic form on their own.
+"""
+import numpy as np
+import pytest
+
+from conftest import min_abs_tilt_index, rel_l2
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL_STAGE = 1e-5
+TOL_SOLVE = 1e-4
+
+
+def _t(a, dtype=None):
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dtype=dtype)
+
+
+@pytest.mark.parametrize("name", ["a", "b", "c", "cli"])
+def test_toeplitz_solve_matches_reference(golden, name):
+    from feilab_b200 import icon
+    z = golden[name]
+    S = int(z["S"])
+    p = icon.IconPlan(int(z["nx"]), int(z["thickness"]), z["tilts"], capacity=S)
+    p.set_operator("toeplitz")
+    A = p.prepare_rhs(_t(z["rows"], torch.float32))
+    sched = tuple(int(v) for v in z["sched"])
+    m = p.solve(A, sched, int(z["data_type"]), float(z["threshold"]))
+    rp = p.reproject(m).cpu().numpy()
+    m = m.cpu().numpy()
+    assert p.omit_index == min_abs_tilt_index(z["tilts"])
+    for s in range(S):
+        assert rel_l2(m[s], z["ref_m"][s]) < TOL_SOLVE, (name, s)
+        assert rel_l2(rp[s], z["ref_reproj"][s]) < TOL_SOLVE, (name, s)
+    p.close()
+
+
+def _exact_iteration(o, w, m0, Ahwb):
+    """One unconstrained iteration with the exact transform (FP64 NDFT):
+    rhat = A^H W A m0 - Ahwb, alpha = |rhat|^2 / sum w |A rhat|^2."""
+    rh = o.ndft_adjoint(w * o.ndft_forward(m0.astype(np.float64))) - Ahwb
+    rtr = float((np.abs(rh) ** 2).sum())
+    rtar = float((w * np.abs(o.ndft_forward(rh)) ** 2).sum())
+    al = rtr / rtar
+    return m0 - al * rh.real, al, rtr
+
+
+@pytest.mark.parametrize("nx,th,tilts", [
+    (37, 23, np.linspace(-47, 52, 11)),
+    (64, 48, np.arange(-60, 61, 4)),
+    (100, 9, np.linspace(-70, 70, 29)),
+    (8, 8, np.array([-30.0, 0.0, 30.0])),
+])
+def test_toeplitz_iteration_matches_exact_transform(nx, th, tilts):
+    from feilab_b200 import icon
+    from oracle.oracle import OraclePlan
+    tilts = np.asarray(tilts, np.float32)
+    o = OraclePlan(nx, th, tilts, "f64")
+    _, w, _ = o.geometry()
+    w = w.astype(np.float64)
+    rng = np.random.default_rng(nx + th)
+    S = 3
+    m0 = rng.standard_normal((S, nx, th)).astype(np.float32)
+    Ahwb = (rng.standard_normal((S, nx, th)) + 1j * rng.standard_normal((S, nx, th))).astype(np.complex64)
+    p = icon.IconPlan(nx, th, tilts, capacity=S)
+    p.set_operator("toeplitz")
+    m1, al, rt = p.solve(_t(Ahwb), (1, 0, 0), 2, 0.0, m0=_t(m0), history=True)
+    m1 = m1.cpu().numpy()
+    for s in range(S):
+        me, ale, rte = _exact_iteration(o, w, m0[s], Ahwb[s].astype(np.complex128))
+        assert rel_l2(m1[s], me) < TOL_STAGE, (nx, th, s)
+        assert abs(al[0, s] - ale) <= TOL_STAGE * abs(ale)
+        assert abs(rt[0, s] - rte) <= TOL_STAGE * abs(rte)
+    p.close()
+
+
+def test_toeplitz_batch_independence_and_determinism(golden):
+    from feilab_b200 import icon
+    z = golden["a"]
+    S = int(z["S"])
+    p = icon.IconPlan(int(z["nx"]), int(z["thickness"]), z["tilts"], capacity=S)
+    p.set_operator("toeplitz")
+    A = p.prepare_rhs(_t(z["rows"], torch.float32))
+    sched = tuple(int(v) for v in z["sched"])
+    m1 = p.solve(A, sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+    m2 = p.solve(A, sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+    assert np.array_equal(m1, m2)
+    for s in range(S):
+        ms = p.solve(A[s:s + 1].contiguous(), sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+        assert np.array_equal(ms[0], m1[s])
+    p.close()
+
+
+def test_toeplitz_switch_back_gives_nufft_result(golden):
+    from feilab_b200 import icon
+    z = golden["b"]
+    S = int(z["S"])
+    p = icon.IconPlan(int(z["nx"]), int(z["thickness"]), z["tilts"], capacity=S)
+    A = p.prepare_rhs(_t(z["rows"], torch.float32))
+    sched = tuple(int(v) for v in z["sched"])
+    m_n = p.solve(A, sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+    p.set_operator("toeplitz")
+    m_t = p.solve(A, sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+    p.set_operator("nufft")
+    m_n2 = p.solve(A, sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+    assert np.array_equal(m_n, m_n2)
+    for s in range(S):
+        assert rel_l2(m_t[s], m_n[s]) < TOL_SOLVE
+    with pytest.raises(KeyError):
+        p.set_operator("other")
+    p.close()
+
+
+def test_toeplitz_per_group_weights_equal_separate_plans(golden):
+    # Two slice groups with different weight vectors (one tilt's nodes at 0 in
+    # the second, as the leave-one-out sweep sets them) give, slice by slice,
+    # what a plan with only that group's weights gives.
+    from feilab_b200 import icon
+    z = golden["c"]
+    nx, th, tilts = int(z["nx"]), int(z["thickness"]), z["tilts"]
+    p = icon.IconPlan(nx, th, tilts, capacity=16)
+    B = p.B
+    _, w = p.geometry()
+    w2 = w.copy()
+    k = 7
+    w2[k * nx:(k + 1) * nx] = 0.0
+    rows = np.repeat(z["rows"][:1], 2 * B, 0)
+    sched = (2, 3, 1)
+    p.set_operator("toeplitz")
+    A = p.prepare_rhs(_t(rows, torch.float32))
+    p.set_group_weights(np.stack([w, w2]))
+    m = p.solve(A, sched, 2, 0.0).cpu().numpy()
+    p.set_group_weights(np.stack([w2, w]))
+    m_sw = p.solve(A, sched, 2, 0.0).cpu().numpy()
+    p.set_group_weights(None)
+    m_plain = p.solve(A, sched, 2, 0.0).cpu().numpy()
+    assert np.array_equal(m[0], m_plain[0])
+    assert np.array_equal(m_sw[B], m_plain[B])
+    assert np.array_equal(m[B], m_sw[0])
+    assert rel_l2(m[B], m[0]) > 1e-3          # the weights matter
+    p.close()
