@@ -8,8 +8,17 @@ Gaussian blobs on a 0.1 background, 61 tilts -60..+60 deg step 2 stored sorted
 by angle, Gaussian noise SNR 0.1, thickness 300, 300 ICON iterations per
 xz-slice (schedule 10,280,10, data type 2, threshold 0).  A step reconstructs
 one batch of SLICES_PER_STEP slices: input stage (1-D row NUFFTs, W, adjoint)
-plus 300 iterations (3 NUFFTs each).  Per step the working set (~20 GB) is far
-larger than the 126 MB L2, so no flush is needed between steps.
+plus 300 iterations.  Per step the working set (~20 GB) is far larger than
+the 126 MB L2, so no flush is needed between steps.
+
+The iterations' normal operator A^H W A is, by default (--operator toeplitz),
+the Toeplitz form: a convolution with the exact kernel of the node set on
+the oversampled grid (two 2-D FFT round trips per iteration, no
+interpolation); with --operator nufft it is the reference's Gaussian-window
+NUFFT pair (three NUFFTs per iteration).  Both are timed in every run (the
+other one over min(K, 5) steps), both carry a parity record against the
+reference and the FP64 oracle, and the NUFFT pair's HBM GB/s comes from the
+nufft run.
 
 value: slices/s with the projection rows already in HBM (device-timed with
 CUDA events on the launch stream, max over ranks).  e2e: the same through
@@ -354,9 +363,9 @@ def run_ours(args):
     except Exception:
         pass
 
-    def timed_device(op):
-        """Device-resident rows in, K timed steps (input stage + schedule),
-        CUDA events on the launch stream, max over ranks."""
+    def timed_device(op, steps):
+        """Device-resident rows in, `steps` timed steps (input stage +
+        schedule), CUDA events on the launch stream, max over ranks."""
         plan.set_operator(op)
         for i in range(args.warmup):
             plan.solve(plan.prepare_rhs(rows[i]), SCHED, DATA_TYPE, THRESHOLD)
@@ -368,7 +377,7 @@ def run_ours(args):
         with ClockSampler(uuid) as clk:
             barrier()
             ev0.record(stream)
-            for i in range(args.warmup, nsteps):
+            for i in range(args.warmup, args.warmup + steps):
                 plan.solve(plan.prepare_rhs(rows[i]), SCHED, DATA_TYPE, THRESHOLD)
             ev1.record(stream)
             barrier()
@@ -376,8 +385,8 @@ def run_ours(args):
         trace = plan.trace_read()
         plan.trace(False)
         t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
-        return {"value": sharding.job_rate(world, S, args.steps, t), "t": t, "trace": trace, "launches": launches,
-                "clocks": clk.summary()}
+        return {"value": sharding.job_rate(world, S, steps, t), "t": t, "steps": steps, "trace": trace,
+                "launches": launches, "clocks": clk.summary()}
 
     h_rows = torch.empty((nsteps, S, len(tilts), NX), dtype=torch.float32, pin_memory=True)
     h_rows.copy_(rows.cpu())
@@ -407,11 +416,14 @@ def run_ours(args):
                 for k, v in trace.items() if v[0] > 0}
 
     peak, peak_kind = measured_peaks()
+    # The headline operator is timed over the K steps, device-resident and end
+    # to end; the other operator over min(K, 5) steps, device-resident.
     ops = [args.operator] + [o for o in ("nufft", "toeplitz") if o != args.operator]
     runs = {}
     for op in ops:
-        runs[op] = timed_device(op)
-        runs[op]["e2e"] = timed_e2e(op)
+        headline = op == args.operator
+        runs[op] = timed_device(op, args.steps if headline else min(args.steps, 5))
+        runs[op]["e2e"] = timed_e2e(op) if headline else None
     head = runs[args.operator]
     value, t_dev, trace, e2e = head["value"], head["t"], head["trace"], head["e2e"]
 
@@ -426,7 +438,7 @@ def run_ours(args):
     tn = runs["nufft"]["trace"]
     fwd_ms = (tn["xpass_fwd"][1] + tn["ypass_fwd"][1] + tn["interp_fin"][1]) / 2.0
     adj_ms = tn["ypass_adj"][1] + tn["xpass_adj"][1]
-    slice_iters = slots * args.steps * sum(SCHED)
+    slice_iters = slots * runs["nufft"]["steps"] * sum(SCHED)
     pair_s = (fwd_ms + adj_ms) / 1e3 / slice_iters
     pair_gbs = PAIR_MODEL_BYTES / pair_s / 1e9
 
@@ -449,7 +461,8 @@ def run_ours(args):
                     "d2h_bytes_per_step": int(S * NX * THICK * 4)},
             "gpu_launches": int(head["launches"]),
             "clocks": head["clocks"],
-            "operators": {op: {"value": r["value"], "e2e": r["e2e"], "ms_per_step": r["t"] / args.steps * 1e3,
+            "operators": {op: {"value": r["value"], "e2e": r["e2e"], "steps": r["steps"],
+                               "ms_per_step": r["t"] / r["steps"] * 1e3,
                                "kernels": kernel_table(r["trace"]), "clocks": r["clocks"]} for op, r in runs.items()}}
     plan.set_operator(args.operator)
     line["warm_start"] = warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S)
@@ -492,12 +505,13 @@ def warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S):
             net.predict(A[s0:s0 + cap], out=m0[s0:s0 + cap])
         return A, m0, plan.solve(A, SCHED, DATA_TYPE, THRESHOLD, m0=m0)
 
+    steps = min(args.steps, 5)
     for i in range(args.warmup):
         step(i)
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for i in range(args.warmup, args.warmup + args.steps):
+    for i in range(args.warmup, args.warmup + steps):
         A, m0, m_warm = step(i)
     e1.record(stream)
     barrier()
@@ -512,7 +526,7 @@ def warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S):
     torch.cuda.synchronize()
     frc = frc_mean(m_warm[:16], m_cold[:16])
     net.close()
-    return {"value": sharding.job_rate(world, S, args.steps, t), "unit": "slices/s",
+    return {"value": sharding.job_rate(world, S, steps, t), "unit": "slices/s", "steps": steps,
             "schedule": "network start + the full reference schedule", "inference_ms_per_slice":
             round(f0.elapsed_time(f1) / S, 4), "frc_vs_cold_min": round(float(frc.min()), 4),
             "heldout_icon_iterations_to_frc_0.99": {"cold": meta.get("icon_iters_to_frc099_cold"),
@@ -524,13 +538,14 @@ def warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S):
 
 
 def run_profile_case(args):
-    """Small case for ncu captures: 16 slices of the workload (inputs and
-    intermediates of each kernel > L2, a few hundred MB on the device), the
-    input stage and 2 iterations; prints the traced kernel times."""
+    """Small case for ncu captures: --profile-slices slices of the workload
+    (32 by default: the grid intermediate of every kernel, 157 MB, is larger
+    than L2; under 1 GB on the device in all), the input stage and 2
+    iterations; prints the traced kernel times."""
     import torch
     from feilab_b200 import icon
     torch.cuda.set_device(0)
-    S = 16
+    S = args.profile_slices
     rows, tilts = make_rows(list(range(S)), "cuda")
     plan = icon.IconPlan(NX, THICK, tilts, capacity=S)
     plan.set_operator(args.operator)
@@ -552,9 +567,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference ICON-GPU leg")
-    ap.add_argument("--operator", default="nufft", choices=["nufft", "toeplitz"],
+    ap.add_argument("--operator", default="toeplitz", choices=["nufft", "toeplitz"],
                     help="normal operator of the headline run (the other is timed beside it)")
     ap.add_argument("--profile", action="store_true", help="run the small ncu case only")
+    ap.add_argument("--profile-slices", type=int, default=32, help="slices of the --profile case")
     args = ap.parse_args()
     if args.profile:
         run_profile_case(args)

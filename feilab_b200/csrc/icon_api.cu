@@ -541,7 +541,7 @@ icon_status ensure_toeplitz(icon_plan *p, cudaStream_t st)
     dim3 grid((p->n1 + icon::kToepTile - 1) / icon::kToepTile, (p->n0 + icon::kToepTile - 1) / icon::kToepTile,
               groups_needed);
     icon::k_toep_kernel<<<grid, 256, 0, st>>>(xy_d, w, p->wgroups > 0 ? (size_t)p->M : 0, p->M, p->N0, p->N1, p->n0,
-                                              p->n1, p->Kt);
+                                              p->n1, icon::ytoep4_fits(p->n1) ? p->lg1 - 5 : 0, p->Kt);
     ICON_CUDA(cudaGetLastError());
     p->kt_groups = groups_needed;
     p->kt_stale = false;

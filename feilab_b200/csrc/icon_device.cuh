@@ -295,6 +295,34 @@ __device__ __forceinline__ void dft_inplace(float2 (&a)[R], float dir)
     if constexpr (R >= 2) dft_stage<R, 2>(a, dir);
 }
 
+// One radix-2 decimation-in-frequency stage (butterfly span LEN), then the
+// next, shorter one.
+template <int R, int LEN>
+__device__ __forceinline__ void dif_stage(float2 (&a)[R], float dir)
+{
+#pragma unroll
+    for (int i = 0; i < R; i += LEN) {
+#pragma unroll
+        for (int k = 0; k < LEN / 2; ++k) {
+            const float2 p = a[i + k], q = a[i + k + LEN / 2];
+            a[i + k] = add2(p, q);
+            const float2 d = sub2(p, q);
+            a[i + k + LEN / 2] = (k == 0) ? d : cmul(w32((k * (32 / LEN)) & 31, dir), d);
+        }
+    }
+    if constexpr (LEN > 2) dif_stage<R, LEN / 2>(a, dir);
+}
+
+// In-place radix-2 DIF DFT of R values held in registers, a[] given in
+// natural order; on return a[brev(q)] = sum_r x[r] exp(dir*2*pi*i*r*q/R)
+// (brev over log2 R bits).  The mirror of dft_inplace: the two compose
+// without a register permutation in between.
+template <int R>
+__device__ __forceinline__ void dft_dif_inplace(float2 (&a)[R], float dir)
+{
+    if constexpr (R >= 2) dif_stage<R, R>(a, dir);
+}
+
 // Position of point p in the intermediate buffer s.  With SWZ, points p and
 // p ^ 1 trade places when bit zs of p is set (zs = log2 of the first pass's
 // radix).  The first pass writes points j*R + r, so with an unpadded stride

@@ -41,10 +41,26 @@ void Launch<B>::xpass_fwd_full(int E, dim3 grid, int threads, size_t smem, cudaS
     else k_xpass_fwd<true, B, 16, true><<<grid, threads, smem, st>>>(g, in, G1);
 }
 
+// The four-step register FFT (k_ytoep4) for n1 = 128 .. 1024; blockDim =
+// n1*B/32, shared memory n1*B float2.
+template <int B, int MODE>
+static void launch_ytoep4(dim3 grid, cudaStream_t st, const Geo &g, float2 *G1, double *part)
+{
+    const int threads = g.n1 * B / 32;
+    const size_t smem = ytoep4_smem(g.n1, B);
+    switch (g.lg1) {
+    case 7: k_ytoep4<B, 2, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    case 8: k_ytoep4<B, 3, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    case 9: k_ytoep4<B, 4, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    default: k_ytoep4<B, 5, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    }
+}
+
 template <int B>
 void Launch<B>::ypass_toep(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g, float2 *G1)
 {
-    if (E == 32) k_ypass_toep<B, 32><<<grid, threads, smem, st>>>(g, G1);
+    if (ytoep4_fits(g.n1)) launch_ytoep4<B, 0>(grid, st, g, G1, nullptr);
+    else if (E == 32) k_ypass_toep<B, 32><<<grid, threads, smem, st>>>(g, G1);
     else k_ypass_toep<B, 16><<<grid, threads, smem, st>>>(g, G1);
 }
 
@@ -52,7 +68,8 @@ template <int B>
 void Launch<B>::ypass_toep_quad(int E, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
                                 const float2 *G1, double *part)
 {
-    if (E == 32) k_ypass_toep_quad<B, 32><<<grid, threads, smem, st>>>(g, G1, part);
+    if (ytoep4_fits(g.n1)) launch_ytoep4<B, 1>(grid, st, g, const_cast<float2 *>(G1), part);
+    else if (E == 32) k_ypass_toep_quad<B, 32><<<grid, threads, smem, st>>>(g, G1, part);
     else k_ypass_toep_quad<B, 16><<<grid, threads, smem, st>>>(g, G1, part);
 }
 
@@ -163,6 +180,14 @@ cudaError_t Launch<B>::set_smem(int ex, int ey, size_t smem_x, size_t need_x, si
         set((const void *)k_rows_fwd<B, 16>, smem_x);
         set((const void *)k_row_adj<B, 16>, smem_x);
     }
+    set((const void *)k_ytoep4<B, 2, 0>, ytoep4_smem(128, B));
+    set((const void *)k_ytoep4<B, 3, 0>, ytoep4_smem(256, B));
+    set((const void *)k_ytoep4<B, 4, 0>, ytoep4_smem(512, B));
+    set((const void *)k_ytoep4<B, 5, 0>, ytoep4_smem(1024, B));
+    set((const void *)k_ytoep4<B, 2, 1>, ytoep4_smem(128, B));
+    set((const void *)k_ytoep4<B, 3, 1>, ytoep4_smem(256, B));
+    set((const void *)k_ytoep4<B, 4, 1>, ytoep4_smem(512, B));
+    set((const void *)k_ytoep4<B, 5, 1>, ytoep4_smem(1024, B));
     if (ey == 32) {
         set((const void *)k_ypass_fwd<B, 32, false>, smem_y);
         set((const void *)k_ypass_fwd<B, 32, true>, smem_y);

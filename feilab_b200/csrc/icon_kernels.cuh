@@ -1085,10 +1085,12 @@ __device__ __forceinline__ double dirichlet(double x, double kn, double sa, doub
 
 #ifndef ICON_KERNELS_TEMPLATES_ONLY
 // xy: [M][2] node coordinates, w: [M] weights (group g's at w + g*wstride for
-// blockIdx.z = g); K: [G][n0][n1] float.
+// blockIdx.z = g); K: [G][n0][n1] float.  With perm_lr > 0 each row is stored
+// in the order k_ytoep4 reads it: frequency k1 of row k0 at
+// (k1 mod R) * 32 + k1 / R, R = 2^perm_lr = n1 / 32.
 __global__ void __launch_bounds__(256) k_toep_kernel(const float *__restrict__ xy, const float *__restrict__ w,
                                                      size_t wstride, int M, int N0, int N1, int n0, int n1,
-                                                     float *__restrict__ K)
+                                                     int perm_lr, float *__restrict__ K)
 {
     __shared__ __align__(16) double F0[kToepNodes][kToepTile];   // w_j D_N0(x_j0 - k0/n0)
     __shared__ __align__(16) double F1[kToepNodes][kToepTile];   // D_N1(x_j1 - k1/n1)
@@ -1160,7 +1162,8 @@ __global__ void __launch_bounds__(256) k_toep_kernel(const float *__restrict__ x
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
             const int k1 = k1b + 4 * tx + jj;
-            if (k0 < n0 && k1 < n1) Kg[(size_t)k0 * n1 + k1] = (float)(acc[i][jj] * scale);
+            const int pos = perm_lr > 0 ? ((k1 & ((1 << perm_lr) - 1)) << 5) + (k1 >> perm_lr) : k1;
+            if (k0 < n0 && k1 < n1) Kg[(size_t)k0 * n1 + pos] = (float)(acc[i][jj] * scale);
         }
     }
 }
@@ -1251,5 +1254,157 @@ __global__ void FFT_BOUNDS(E) k_ypass_toep_quad(Geo g, const float2 *__restrict_
     const double r = block_sum_per_slice(st.acc, red, B);
     if ((int)threadIdx.x < B) part[((size_t)grp * g.n0 + x) * B + threadIdx.x] = r;
 }
+
+// ------------------------------------------- Toeplitz y-passes, 4-step ----
+// The y-direction transforms of the Toeplitz passes for n1 = 32 R
+// (R = 2^LR, 2 <= R <= 32) as a four-step FFT held in registers.  With
+// y = 32 a + c (a < R, c < 32) and k = k1 + R k2 (k1 < R, k2 < 32):
+//   X[k1 + R k2] = sum_c w32^(c k2) [ wn^(c k1) sum_a x[32 a + c] wR^(a k1) ],
+// w_L = exp(-2 pi i / L).  A thread of slice b owns 32 values: first the
+// 32/R R-point DFTs over a of its columns c = u + R i, then, after one
+// transpose through shared memory, the 32-point DFT over c of its k1 = u.
+// It then holds X[k1 + R k2] for every k2: a strided set of frequencies,
+// which is all that the pointwise product with K and the quadratic form
+// need.  The inverse runs the same steps backwards from there (32-point
+// inverse DFT, conjugate twiddles, one transpose, R-point inverse DFTs), so
+// the forward-multiply-inverse round trip takes two transposes and no
+// reordering pass.  The N1 inputs of a row are loaded from global memory
+// straight into registers (the B slices of a point are B consecutive float2,
+// so a warp reads 256 contiguous bytes) and the N1 outputs stored from
+// registers; the zero padding is never loaded.  Shared memory holds only the
+// transposed [32][R][B] values, with k1 XOR-swizzled by the low bits of c so
+// that both the column-wise writes and the row-wise reads of a warp are
+// conflict-free (two wavefronts per 32 x 8 bytes).  Each slice's values stay
+// its own, so a slice's result does not depend on its group mates.
+template <int B, int LR>
+__device__ __forceinline__ int ytoep4_sidx(int c, int k1, int b)
+{
+    constexpr int R = 1 << LR;
+    constexpr int SWM = (R - 1) & (16 / B - 1);
+    return ((c * R + (k1 ^ (c & SWM))) << Log2B<B>::v) + b;
+}
+
+// MODE 0: row x of G1 <- crop F^-1(K[x][.] . F(pad row)), in place (the
+// Toeplitz y-pass of A^H W A m).  MODE 1: part[G][n0][B] <- per slice
+// sum_k K[x][k] |F(pad row)[k]|^2 in FP64 (the step length's denominator).
+template <int B, int LR, int MODE>
+__global__ void __launch_bounds__((1 << LR) * B, 512 / ((1 << LR) * B) < 32 ? 512 / ((1 << LR) * B) : 32)
+    k_ytoep4(Geo g, float2 *__restrict__ G1, double *__restrict__ part)
+{
+    constexpr int R = 1 << LR;
+    constexpr int LB = Log2B<B>::v;
+    constexpr int NI = 32 / R;
+    extern __shared__ float2 s[];
+    const int grp = blockIdx.x, x = blockIdx.y, N1 = g.N1;
+    const int t = threadIdx.x, b = t & (B - 1), u = t >> LB;
+    float2 *row = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
+    const float *krow = g.Kt + grp * g.kstride + (size_t)x * (32 * R);
+
+    // Step 1: R-point DFTs over a, twiddles wn^(c k1), transpose.
+    {
+        float2 v[NI][R];
+#pragma unroll
+        for (int i = 0; i < NI; ++i) {
+            const int c = u + R * i;
+            const float2 *rb = row + (c * B + b);   // point y = 32 a + c at rb[32 B a]
+            const int na = (N1 - c + 31) >> 5;      // points y < N1
+#pragma unroll
+            for (int a = 0; a < R; ++a)
+                v[i][brev5(a) >> (5 - LR)] = a < na ? rb[32 * B * a] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int i = 0; i < NI; ++i) {
+            const int c = u + R * i;
+            dft_inplace<R>(v[i], -1.f);
+            // wn^(c k1): from the table at k1 = 0, 8, 16, 24, stepped by
+            // wn^c in between (at most 7 products from a table value).
+            const float2 w1 = __ldg(&g.tw1[c]);
+            float2 tw = w1;
+#pragma unroll
+            for (int k1 = 1; k1 < R; ++k1) {
+                if ((k1 & 7) == 0) tw = __ldg(&g.tw1[c * k1]);
+                else if (k1 > 1) tw = cmul(tw, w1);
+                v[i][k1] = cmul(v[i][k1], tw);
+            }
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) s[ytoep4_sidx<B, LR>(c, k1, b)] = v[i][k1];
+        }
+    }
+    __syncthreads();
+    // Step 2: 32-point DFT over c for k1 = u: w[k2] = X[u + R k2].
+    float2 w[32];
+#pragma unroll
+    for (int c = 0; c < 32; ++c) w[brev5(c)] = s[ytoep4_sidx<B, LR>(c, u, b)];
+    dft_inplace<32>(w, -1.f);
+    // K[x][u + R k2] for k2 = 0..31: 32 consecutive floats of the permuted row.
+    const float4 *kq = reinterpret_cast<const float4 *>(krow + 32 * u);
+    if constexpr (MODE == 1) {
+        double acc = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float4 k4 = __ldg(&kq[q]);
+            const float kv[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float2 a = w[4 * q + j];
+                acc += (double)kv[j] * ((double)a.x * (double)a.x + (double)a.y * (double)a.y);
+            }
+        }
+        __syncthreads();   // every read of s is done before the reduction reuses it
+        const double r = block_sum_per_slice(acc, reinterpret_cast<double *>(s), B);
+        if (t < B) part[((size_t)grp * g.n0 + x) * B + t] = r;
+    } else {
+        // Pointwise product with K, 32-point inverse DFT over k2, twiddles
+        // conj(wn^(c k1)), transpose back.
+        // In place: w[k2] *= K, then the DIF inverse leaves Z[c] at w[brev5(c)].
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float4 k4 = __ldg(&kq[q]);
+            const float kv[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) w[4 * q + j] = make_float2(w[4 * q + j].x * kv[j], w[4 * q + j].y * kv[j]);
+        }
+        dft_dif_inplace<32>(w, +1.f);
+        {
+            // conj(wn^(c u)), table at c = 0, 8, 16, 24, products between.
+            float2 w1 = __ldg(&g.tw1[u]);
+            w1.y = -w1.y;
+            float2 tw = w1;
+#pragma unroll
+            for (int c = 1; c < 32; ++c) {
+                if ((c & 7) == 0) {
+                    tw = __ldg(&g.tw1[c * u]);
+                    tw.y = -tw.y;
+                } else if (c > 1) {
+                    tw = cmul(tw, w1);
+                }
+                w[brev5(c)] = cmul(w[brev5(c)], tw);
+            }
+        }
+        __syncthreads();   // every read of s is done before it is overwritten
+#pragma unroll
+        for (int c = 0; c < 32; ++c) s[ytoep4_sidx<B, LR>(c, u, b)] = w[brev5(c)];
+        __syncthreads();
+        // R-point inverse DFTs over k1 for columns c = u + R i; rows y < N1 out.
+#pragma unroll
+        for (int i = 0; i < NI; ++i) {
+            const int c = u + R * i;
+            float2 v[R];
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) v[brev5(k1) >> (5 - LR)] = s[ytoep4_sidx<B, LR>(c, k1, b)];
+            dft_inplace<R>(v, +1.f);
+            float2 *rb = row + (c * B + b);
+            const int na = (N1 - c + 31) >> 5;
+#pragma unroll
+            for (int a = 0; a < R; ++a)
+                if (a < na) rb[32 * B * a] = v[a];
+        }
+    }
+}
+
+// Shared memory of k_ytoep4: the transposed [32][R][B] values.
+__host__ __device__ inline size_t ytoep4_smem(int n1, int B) { return (size_t)n1 * B * sizeof(float2); }
+// n1 sizes k_ytoep4 takes (R = n1 / 32 from 4 to 32).
+__host__ __device__ inline bool ytoep4_fits(int n1) { return n1 >= 128 && n1 <= 1024; }
 
 }  // namespace icon

@@ -148,3 +148,34 @@ def test_toeplitz_per_group_weights_equal_separate_plans(golden):
     assert np.array_equal(m[B], m_sw[0])
     assert rel_l2(m[B], m[0]) > 1e-3          # the weights matter
     p.close()
+
+
+@pytest.mark.parametrize("nx,th,ntilt", [
+    (1024, 160, 31),    # 8-slice groups, 512-point y transforms
+    (512, 257, 21),     # 8-slice groups, 1024-point y transforms
+    (2048, 200, 21),    # 4-slice groups (oversampled width 4096)
+    (4096, 100, 11),    # 2-slice groups (oversampled width 8192), 256-point y transforms
+])
+def test_toeplitz_iteration_matches_nufft_iteration_at_large_shapes(nx, th, ntilt):
+    # One iteration from a random start with both normal operators: they are
+    # the same operator up to the Gaussian window's error (~1e-6 relative),
+    # so m, alpha and ||rhat||^2 agree to 1e-5.  Covers the group sizes and
+    # y-transform lengths that the fixtures above do not reach.
+    from feilab_b200 import icon
+    tilts = np.linspace(-60, 60, ntilt).astype(np.float32)
+    p = icon.IconPlan(nx, th, tilts, capacity=4)
+    rng = np.random.default_rng(nx + th)
+    S = 3
+    m0 = rng.standard_normal((S, nx, th)).astype(np.float32)
+    Ahwb = (rng.standard_normal((S, nx, th)) + 1j * rng.standard_normal((S, nx, th))).astype(np.complex64)
+    res = {}
+    for op in ("nufft", "toeplitz"):
+        p.set_operator(op)
+        m1, al, rt = p.solve(_t(Ahwb), (1, 0, 0), 2, 0.0, m0=_t(m0), history=True)
+        res[op] = (m1.cpu().numpy(), al, rt)
+    (mn, aln, rtn), (mt, alt, rtt) = res["nufft"], res["toeplitz"]
+    for s in range(S):
+        assert rel_l2(mt[s], mn[s]) < TOL_STAGE, (nx, th, s)
+        assert abs(alt[0, s] - aln[0, s]) <= TOL_STAGE * abs(aln[0, s])
+        assert abs(rtt[0, s] - rtn[0, s]) <= TOL_STAGE * abs(rtn[0, s])
+    p.close()
