@@ -195,12 +195,23 @@ struct icon_plan {
     // Normal operator of the iterations: ICON_OPERATOR_NUFFT (the reference's
     // NUFFT pair) or ICON_OPERATOR_TOEPLITZ (A^H W A as a convolution with Kt).
     int op = ICON_OPERATOR_NUFFT;
+    // Tolerance stop of the reconstruct calls (icon_plan_set_stop): 0 = the
+    // full schedule.
+    double stop_tol = 0.0;
+    int stop_every = 10;
     float *Kt = nullptr;        // [Gcap][n0][n1] Toeplitz kernels (one used unless per-group weights)
     int kt_groups = 0;          // kernels computed for: 1 = the plan's weights, Gcap = per-group weights
     bool kt_stale = true;
     float *ones0 = nullptr, *ones1 = nullptr;   // unit deapodisation of the Toeplitz x-passes
     size_t smem_yt = 0;
     int na_rtar = 0;            // partial sums per group of the step length's denominator
+    // Toeplitz iterations with the three-step x-kernels (k_xtoep) defer each
+    // iteration's update m -= alpha Re r-hat into the next iteration's forward
+    // x-pass; flush_update applies a pending one where the loop ends.
+    bool xt_ok = false;         // k_xtoep has a variant for n0
+    bool upd_pending = false, upd_clamp = false;
+    int upd_dtype = 0, upd_G = 0;
+    float upd_thr = 0.f;
     int k3_blocks = 0;
     // reprojection lines, keyed by the .tlt angle
     std::map<float, std::unique_ptr<NodeTables>> lines;
@@ -275,7 +286,7 @@ struct icon_plan {
 
 namespace {
 
-enum Kind { K_XF = 0, K_YF, K_FIN, K_YA, K_XA, K_ALPHA, K_UPD, K_ROWS, K_LAYOUT, K_ROWADJ, K_YT, K_YQ };
+enum Kind { K_XF = 0, K_YF, K_FIN, K_YA, K_XA, K_ALPHA, K_UPD, K_ROWS, K_LAYOUT, K_ROWADJ, K_YT, K_YQ, K_XTF, K_XTM };
 
 // Launches one kernel; counts it and, while tracing, brackets it by events
 // and records its algorithmic bytes (compulsory reads + writes, see
@@ -548,12 +559,65 @@ icon_status ensure_toeplitz(icon_plan *p, cudaStream_t st)
     return ICON_OK;
 }
 
+// Applies a deferred update (m -= alpha Re r-hat, clamped as recorded) of
+// the last Toeplitz iteration, if one is pending.
+icon_status flush_update(icon_plan *p, cudaStream_t st)
+{
+    if (!p->upd_pending) return ICON_OK;
+    p->upd_pending = false;
+    const int G = p->upd_G;
+    int per_group = p->N1 * p->N0 * p->B;
+    dim3 gu((unsigned)std::min<size_t>(((size_t)per_group + 255) / 256, 512), G);
+    WITH_B(p->B, LAUNCH_B(p, K_UPD, st, stage_bytes(p, p->nodes).upd * G * p->B,
+                          L::update(gu, st, p->m, p->rhat, p->alpha, per_group, p->upd_clamp ? 1 : 0, p->upd_dtype,
+                                    p->upd_thr)))
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+// One Toeplitz iteration with the three-step x-kernels: the forward x-pass of
+// m (applying the previous iteration's deferred update first), the Toeplitz
+// y-pass, the fused inverse x-pass / r-hat / forward x-pass of r-hat, the
+// quadratic form's y-pass and the step length.  This iteration's update is
+// left pending (flush_update or the next iteration applies it).
+icon_status launch_iteration_xt(icon_plan *p, int G, bool clamp, int data_type, float thr, double *hist_a,
+                                double *hist_r, cudaStream_t st)
+{
+    if (p->upd_pending && p->upd_G != G) ICON_TRY(flush_update(p, st));
+    Geo g = p->geo_unit();
+    const double slots = (double)G * p->B;
+    const double NN = (double)p->N0 * p->N1, G1b = (double)p->n0 * p->N1 * 8, Kb = (double)p->n0 * p->n1 * 4;
+    icon::XtArgs xa{};
+    xa.N0 = p->N0; xa.N1 = p->N1; xa.n0 = p->n0; xa.tw0 = p->tw0; xa.G1 = p->G1; xa.m = p->m;
+    xa.rhat_in = p->rhat; xa.alpha = p->alpha; xa.upd = p->upd_pending ? 1 : 0; xa.clamp = p->upd_clamp ? 1 : 0;
+    xa.data_type = p->upd_dtype; xa.thr = p->upd_thr; xa.rhat = p->rhat; xa.Ahwb = p->Ahwb; xa.part_rtr = p->part_rtr;
+    const double xf_bytes = (xa.upd ? NN * 16 : NN * 4) + G1b;
+    dim3 gy(G, p->n0);
+    WITH_B(p->B,
+        LAUNCH_B(p, K_XTF, st, xf_bytes * slots, L::xtoep(0, st, G, xa));
+        LAUNCH_B(p, K_YT, st, (2 * G1b) * slots + Kb * G, L::ypass_toep(p->ey, gy, p->thr_y, p->smem_yt, st, g, p->G1));
+        LAUNCH_B(p, K_XTM, st, (2 * G1b + NN * 16) * slots, L::xtoep(1, st, G, xa));
+        LAUNCH_B(p, K_YQ, st, G1b * slots + Kb * G,
+                 L::ypass_toep_quad(p->ey, gy, p->thr_y, p->smem_yt, st, g, p->G1, p->part_rtar)))
+    LAUNCH(p, K_ALPHA, st, icon::k_alpha<<<G, 32 * p->B, 0, st>>>(p->part_rtr, p->N1, p->part_rtar, p->n0, p->B, p->alpha, hist_a, hist_r));
+    ICON_CUDA(cudaGetLastError());
+    p->upd_pending = true;
+    p->upd_clamp = clamp;
+    p->upd_dtype = data_type;
+    p->upd_thr = thr;
+    p->upd_G = G;
+    return ICON_OK;
+}
+
 // One ICON iteration with A^H W A as a convolution (k_ypass_toep): the same
 // steps as launch_iteration, f-hat = A^H W A m and rtar = r^H A^H W A r
-// taken from the Toeplitz form instead of the NUFFT pair.
+// taken from the Toeplitz form instead of the NUFFT pair.  With the
+// three-step x-kernels and no step measurement it is launch_iteration_xt.
 icon_status launch_iteration_toep(icon_plan *p, int G, bool clamp, int data_type, float thr, double *hist_a,
                                   double *hist_r, cudaStream_t st, bool measure_step)
 {
+    if (p->xt_ok && !measure_step) return launch_iteration_xt(p, G, clamp, data_type, thr, hist_a, hist_r, st);
+    ICON_TRY(flush_update(p, st));
     Geo g = p->geo_unit();
     const double slots = (double)G * p->B;
     const double NN = (double)p->N0 * p->N1, G1b = (double)p->n0 * p->N1 * 8, Kb = (double)p->n0 * p->n1 * 4;
@@ -581,18 +645,65 @@ icon_status launch_iteration_toep(icon_plan *p, int G, bool clamp, int data_type
     return ICON_OK;
 }
 
-// After the row transform of G groups: Ahwb = A^H W b, m = 0, the schedule's
-// iterations (MainCode.cu:115-140 with Iteration3).
-icon_status solve_from_rows(icon_plan *p, const icon_solve_cfg *cfg, int G, cudaStream_t st)
+// The schedule (Iteration2.cu:129-132) on the plan's m for G groups of which
+// the first S slices count, with the ICON phase ended once every one of
+// those slices' relative step ||m_new - m_old|| / ||m_new|| is at or below
+// tol (checked every check_every ICON iterations and at the phase's last;
+// each check synchronises the stream).  *done receives the iterations run
+// and h_step (optional) the slices' steps at the last check.
+icon_status run_schedule_tol(icon_plan *p, const icon_solve_cfg *cfg, int G, int S, double tol, int check_every,
+                             int *done_out, double *h_step, cudaStream_t st)
+{
+    const int a = cfg->infr_before, b = cfg->icon, c = cfg->infr_after;
+    const size_t slots = (size_t)G * p->B;
+    std::vector<double> hs(slots);
+    icon_status rc = ICON_OK;
+    int done = 0;
+    p->upd_pending = false;
+    auto run = [&](int n, bool clamp, bool checked) {
+        for (int k = 0; k < n && rc == ICON_OK; ++k) {
+            const bool check = checked && ((k + 1) % check_every == 0 || k + 1 == n);
+            rc = launch_iteration(p, G, clamp, cfg->data_type, cfg->threshold, nullptr, nullptr, st, check);
+            ++done;
+            if (rc != ICON_OK || !check) continue;
+            cudaError_t e = cudaMemcpyAsync(hs.data(), p->step, sizeof(double) * slots, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) {
+                rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
+                break;
+            }
+            bool all = true;
+            for (int s = 0; s < S; ++s) {
+                if (h_step) h_step[s] = hs[s];
+                if (!(hs[s] <= tol)) all = false;
+            }
+            if (all) break;
+        }
+    };
+    run(a, false, false);   // INFR (Iteration2.cu:129-132)
+    run(b, true, true);     // ICON, stopped once every slice's step is within tol
+    run(c, false, false);   // INFR
+    if (rc == ICON_OK) rc = flush_update(p, st);
+    p->upd_pending = false;
+    if (done_out) *done_out = done;
+    return rc;
+}
+
+// After the row transform of G groups (Sc slices): Ahwb = A^H W b, m = 0,
+// the schedule's iterations (MainCode.cu:115-140 with Iteration3), ended at
+// the plan's tolerance when one is set (icon_plan_set_stop).
+icon_status solve_from_rows(icon_plan *p, const icon_solve_cfg *cfg, int G, int Sc, cudaStream_t st)
 {
     const int a = cfg->infr_before, b = cfg->icon, c = cfg->infr_after, iters = a + b + c;
     ICON_TRY(ensure_toeplitz(p, st));
     ICON_TRY(launch_adjoint(p, p->f, G, 0, p->Ahwb, st));
     size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
     ICON_CUDA(cudaMemsetAsync(p->m, 0, tot * sizeof(float), st));
+    if (p->stop_tol > 0.0) return run_schedule_tol(p, cfg, G, Sc, p->stop_tol, p->stop_every, nullptr, nullptr, st);
+    p->upd_pending = false;
     for (int it = 0; it < iters; ++it)
         ICON_TRY(launch_iteration(p, G, a <= it && it < iters - c, cfg->data_type, cfg->threshold, nullptr, nullptr, st));
-    return ICON_OK;
+    return flush_update(p, st);
 }
 
 icon_status line_tables(icon_plan *p, float tilt_deg, NodeTables **out)
@@ -757,6 +868,9 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
         cudaError_t e = cudaSuccess;
         WITH_B(B, e = L::set_smem(p->ex, p->ey, p->smem_x, need_x, p->smem_y, p->smem_ya, p->smem_yt))
         if (e != cudaSuccess) return fail(ICON_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        WITH_B(B, e = L::xtoep_prepare(p->n0))
+        if (e != cudaSuccess) return fail(ICON_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        p->xt_ok = p->n0 >= 128 && p->n0 <= 8192 && (size_t)smem_max >= icon::xtoep_smem(p->n0, std::min(B, 8192 / p->n0));
     }
     // Scratch for Gcap groups.
     size_t G = p->Gcap, Bz = B;
@@ -851,6 +965,15 @@ icon_status icon_plan_set_group_weights(icon_plan *p, const float *h_w, int ngro
         ICON_CUDA(cudaMemcpy(p->wgroup + gi * M, p->nodes.w, sizeof(float) * M, cudaMemcpyDeviceToDevice));
     p->wgroups = ngroups;
     p->kt_stale = true;
+    return ICON_OK;
+}
+
+icon_status icon_plan_set_stop(icon_plan *p, double tol, int check_every)
+{
+    if (!p) return fail(ICON_ERR_INVALID, "null plan");
+    if (!(tol >= 0.0) || check_every < 1) return fail(ICON_ERR_INVALID, "tol must be >= 0 and check_every >= 1");
+    p->stop_tol = tol;
+    p->stop_every = check_every;
     return ICON_OK;
 }
 
@@ -980,7 +1103,7 @@ icon_status icon_reconstruct_stack(icon_plan *p, const icon_solve_cfg *cfg, cons
     for (int s0 = 0; s0 < S; s0 += p->cap) {
         const int Sc = std::min(p->cap, S - s0), G = groups(p, Sc);
         ICON_TRY(launch_rows_at(p, d_stack + (size_t)(y0 + s0) * nx, nx, (size_t)ny * nx, skip, Sc, G, nullptr, st));
-        ICON_TRY(solve_from_rows(p, cfg, G, st));
+        ICON_TRY(solve_from_rows(p, cfg, G, Sc, st));
         if (d_slices) {
             dim3 gl((unsigned)std::min<size_t>(((size_t)G * NN + 255) / 256, 4096));
             WITH_B(p->B, LAUNCH(p, K_LAYOUT, st, L::img_out_file(gl, st, p->m, d_slices + (size_t)s0 * NN, Sc, p->N0, p->N1)))
@@ -1120,12 +1243,15 @@ icon_status icon_solve(icon_plan *p, const icon_solve_cfg *cfg, const void *d_Ah
     bool want_hist = (h_alpha || h_rtr) && iters > 0;
     if (want_hist) ICON_CUDA(cudaMalloc(&hist, sizeof(double) * 2 * slots * iters));
     icon_status rc = ICON_OK;
+    p->upd_pending = false;
     for (int it = 0; it < iters && rc == ICON_OK; ++it) {
         bool clamp = (a <= it && it < iters - c);              // Iteration2.cu:129
         double *ha = want_hist ? hist + (size_t)it * slots : nullptr;
         double *hr = want_hist ? hist + (size_t)(iters + it) * slots : nullptr;
         rc = launch_iteration(p, G, clamp, cfg->data_type, cfg->threshold, ha, hr, st);
     }
+    if (rc == ICON_OK) rc = flush_update(p, st);
+    p->upd_pending = false;
     if (rc == ICON_OK) {
         LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float><<<grid1d((size_t)S * p->N0 * p->N1), 256, 0, st>>>(p->m, d_m, S, p->N0, p->N1, p->B));
         cudaError_t e = cudaGetLastError();
@@ -1163,32 +1289,8 @@ icon_status icon_solve_until(icon_plan *p, const icon_solve_cfg *cfg, const void
     LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float2><<<grid1d(tot), 256, 0, st>>>((const float2 *)d_Ahwb, p->Ahwb, S, p->N0, p->N1, p->B, tot));
     if (warm_start) LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float><<<grid1d(tot), 256, 0, st>>>(d_m, p->m, S, p->N0, p->N1, p->B, tot));
     else ICON_CUDA(cudaMemsetAsync(p->m, 0, tot * sizeof(float), st));
-    std::vector<double> hs(slots);
-    icon_status rc = ICON_OK;
     int done = 0;
-    auto run = [&](int n, bool clamp, bool checked) {
-        for (int k = 0; k < n && rc == ICON_OK; ++k) {
-            const bool check = checked && ((k + 1) % check_every == 0 || k + 1 == n);
-            rc = launch_iteration(p, G, clamp, cfg->data_type, cfg->threshold, nullptr, nullptr, st, check);
-            ++done;
-            if (rc != ICON_OK || !check) continue;
-            cudaError_t e = cudaMemcpyAsync(hs.data(), p->step, sizeof(double) * slots, cudaMemcpyDeviceToHost, st);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess) {
-                rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e));
-                break;
-            }
-            bool all = true;
-            for (int s = 0; s < S; ++s) {
-                if (h_step) h_step[s] = hs[s];
-                if (!(hs[s] <= tol)) all = false;
-            }
-            if (all) break;
-        }
-    };
-    run(a, false, false);   // INFR (Iteration2.cu:129-132)
-    run(b, true, true);     // ICON, stopped once every slice's step is within tol
-    run(c, false, false);   // INFR
+    icon_status rc = run_schedule_tol(p, cfg, G, S, tol, check_every, &done, h_step, st);
     if (rc == ICON_OK) {
         LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float><<<grid1d((size_t)S * p->N0 * p->N1), 256, 0, st>>>(p->m, d_m, S, p->N0, p->N1, p->B));
         cudaError_t e = cudaGetLastError();
@@ -1196,6 +1298,24 @@ icon_status icon_solve_until(icon_plan *p, const icon_solve_cfg *cfg, const void
     }
     if (h_iters) *h_iters = done;
     return rc;
+}
+
+icon_status icon_reproject_host(icon_plan *p, const float *h_m, float tilt_deg, float *h_out, int S, void *stream)
+{
+    if (!p) return fail(ICON_ERR_INVALID, "null plan");
+    if (!h_m || !h_out) return fail(ICON_ERR_INVALID, "null buffer");
+    if (S < 1) return fail(ICON_ERR_INVALID, "S must be >= 1");
+    DeviceGuard guard(p->dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t NN = (size_t)p->N0 * p->N1, nx = p->nx;
+    for (int s0 = 0; s0 < S; s0 += p->cap) {
+        const int Sc = std::min(p->cap, S - s0);
+        ICON_CUDA(cudaMemcpyAsync(p->mout, h_m + (size_t)s0 * NN, sizeof(float) * NN * Sc, cudaMemcpyHostToDevice, st));
+        ICON_TRY(icon_reproject(p, p->mout, tilt_deg, p->outrp, Sc, st));
+        ICON_CUDA(cudaMemcpyAsync(h_out + (size_t)s0 * nx, p->outrp, sizeof(float) * nx * Sc, cudaMemcpyDeviceToHost, st));
+        ICON_CUDA(cudaStreamSynchronize(st));
+    }
+    return ICON_OK;
 }
 
 icon_status icon_reproject(icon_plan *p, const float *d_m, float tilt_deg, float *d_out, int S, void *stream)
@@ -1230,7 +1350,7 @@ icon_status icon_reconstruct_host(icon_plan *p, const icon_solve_cfg *cfg, const
         cudaError_t e = cudaMemcpyAsync(p->rows, h_rows + (size_t)s0 * R, sizeof(float) * R * Sc, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) { rc = fail(ICON_ERR_CUDA, cudaGetErrorString(e)); break; }
         if ((rc = launch_rows(p, p->rows, Sc, G, nullptr, st)) != ICON_OK) break;
-        if ((rc = solve_from_rows(p, cfg, G, st)) != ICON_OK) break;
+        if ((rc = solve_from_rows(p, cfg, G, Sc, st)) != ICON_OK) break;
         LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float><<<grid1d((size_t)Sc * NN), 256, 0, st>>>(p->m, d_mo, Sc, p->N0, p->N1, p->B));
         if (h_reproj && (rc = reproject_internal(p, p->m, p->reproj_deg, p->outrp, Sc, st)) != ICON_OK) break;
         if ((e = cudaMemcpyAsync(h_m + (size_t)s0 * NN, d_mo, sizeof(float) * NN * Sc, cudaMemcpyDeviceToHost, st)) != cudaSuccess) {

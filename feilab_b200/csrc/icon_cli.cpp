@@ -43,7 +43,12 @@ void help()
     printf("-gpu (-g) : the GPUs to use, e.g. 0,2,4,6; default -1, all GPUs.\n######\n");
     printf("-help (-h) : for help.\n");
     printf("long options: --volume FILE (write the slices as one MRC volume), --batch N (slices per GPU batch, default 128),\n"
-           "  --loo (cross-validate every tilt in turn: crossValidation/loo/tiltNNN.frc and loo_summary.txt)\n");
+           "  --loo (cross-validate every tilt in turn: crossValidation/loo/tiltNNN.frc and loo_summary.txt),\n"
+           "  --operator nufft|toeplitz (normal operator of the iterations: the Gaussian-window NUFFT pair, default,\n"
+           "    or its Toeplitz form, the exact operator as one convolution: faster, within 1e-4 of the default),\n"
+           "  --tol T (end the ICON iterations of a batch once every slice's relative step is at most T; default 0,\n"
+           "    the full -iter schedule), --resume (keep the slices whose reconstruction/mid%%05d.mrc already exists\n"
+           "    with this run's sizes; they are read back, not recomputed)\n");
 }
 
 struct Args {
@@ -57,6 +62,9 @@ struct Args {
     std::vector<int> gpus;
     int batch = 128;
     bool loo = false;
+    int op = ICON_OPERATOR_NUFFT;
+    double tol = 0.0;
+    bool resume = false;
 };
 
 // Per-GPU work: a contiguous slice range.
@@ -74,6 +82,7 @@ std::string join(const std::string &a, const std::string &b) { return a + "/" + 
 // written straight from the pinned buffer while the GPU solves the next batch.
 struct FullSink {
     const Job *job;
+    int ybase;   // slice index of the stack row the batches count from
     const Args *A;
     const MrcHeader *inh;
     int thickness;
@@ -92,7 +101,7 @@ int full_sink(void *ctx, int s0, int count, const float *h_slices, const float *
     double dt = std::chrono::duration<double>(now - c.last).count() / count;
     c.last = now;
     for (int s = 0; s < count; ++s) {
-        const int y = c.job->y0 + s0 + s;
+        const int y = c.ybase + s0 + s;
         const float *slice = h_slices + (size_t)s * NN;
         MrcHeader oh = *c.inh;                           // saveMRC_real.cu:37-46
         oh.mz = c.inh->mx;
@@ -150,19 +159,72 @@ void run_job(Job &job, const Args &A, const MrcHeader &inh, const std::vector<fl
         float *p;
         ~Free() { icon_device_free(dev, p); }
     } free_stack{job.device, d_stack};
-    // Full reconstruction (Lib_2D2, MainCode.cu:3-177).
+    // Full reconstruction (Lib_2D2, MainCode.cu:3-177), in runs of slices
+    // still to do (all of them unless --resume found finished ones).
     {
         icon_geometry g{nx, thickness, nz, tilts.data(), cap, job.device};
         icon_plan *plan = nullptr;
         if (icon_plan_create(&g, &plan) != ICON_OK) return fail("plan");
-        FullSink sink{&job, &A, &inh, thickness, &recdir, volume, &rp_full, std::chrono::steady_clock::now(), {}};
-        icon_status rc = icon_reconstruct_stack_host(plan, &cfg, d_stack, S, 0, -1, S,
-                                                     ICON_OUT_SLICES | ICON_OUT_REPROJECTION, full_sink, &sink, nullptr);
-        icon_plan_destroy(plan);
-        if (rc != ICON_OK) {
-            job.rc = 1;
-            job.err = sink.err.empty() ? std::string("reconstruction: ") + icon_last_error() : sink.err;
-            return;
+        struct Destroy {
+            icon_plan *p;
+            ~Destroy() { icon_plan_destroy(p); }
+        } destroy{plan};
+        if (icon_plan_set_operator(plan, A.op) != ICON_OK || icon_plan_set_stop(plan, A.tol, 10) != ICON_OK)
+            return fail("plan options");
+        std::vector<char> done(S, 0);
+        if (A.resume) {
+            // A finished slice: its file exists with this run's sizes; its
+            // data fills the volume and its reprojection is recomputed.
+            std::vector<float> mine;   // finished slices, [k][N0][N1] (Y fastest)
+            std::vector<int> ys;
+            const size_t NN = (size_t)nx * thickness;
+            std::vector<float> buf;
+            for (int s = 0; s < S; ++s) {
+                char name[64];
+                snprintf(name, sizeof name, "mid%05d.mrc", job.y0 + s);
+                MrcHeader h;
+                std::string e;
+                if (!mrc_read_header(join(recdir, name), h, e) || h.nx != nx || h.ny != thickness || h.nz != 1 ||
+                    h.mode != 2)
+                    continue;
+                buf.resize(NN);
+                if (!mrc_read_sections_into(join(recdir, name), h, 0, 1, buf.data(), e)) continue;
+                done[s] = 1;
+                ys.push_back(job.y0 + s);
+                if (volume) std::memcpy(&(*volume)[(size_t)(job.y0 + s - A.ystart) * NN], buf.data(), sizeof(float) * NN);
+                const size_t k = mine.size() / NN;
+                mine.resize(mine.size() + NN);
+                for (int X = 0; X < nx; ++X)
+                    for (int Y = 0; Y < thickness; ++Y) mine[k * NN + (size_t)X * thickness + Y] = buf[(size_t)Y * nx + X];
+            }
+            if (!ys.empty()) {
+                // Their reprojections at the smallest-|angle| tilt, as the solve's own.
+                std::vector<float> rp(ys.size() * (size_t)nx);
+                if (icon_reproject_host(plan, mine.data(), tilts[omit], rp.data(), (int)ys.size(), nullptr) != ICON_OK)
+                    return fail("reprojection of finished slices");
+                for (size_t k = 0; k < ys.size(); ++k)
+                    std::memcpy(&rp_full[(size_t)(ys[k] - A.ystart) * nx], &rp[k * nx], sizeof(float) * nx);
+                printf("resume: %zu of %d slices on GPU %d already reconstructed\n", ys.size(), S, job.device);
+            }
+        }
+        FullSink sink{&job, job.y0, &A, &inh, thickness, &recdir, volume, &rp_full, std::chrono::steady_clock::now(), {}};
+        for (int r0 = 0; r0 < S;) {
+            if (done[r0]) {
+                ++r0;
+                continue;
+            }
+            int r1 = r0;
+            while (r1 < S && !done[r1]) ++r1;
+            sink.ybase = job.y0 + r0;
+            icon_status rc = icon_reconstruct_stack_host(plan, &cfg, d_stack, S, r0, -1, r1 - r0,
+                                                         ICON_OUT_SLICES | ICON_OUT_REPROJECTION, full_sink, &sink,
+                                                         nullptr);
+            if (rc != ICON_OK) {
+                job.rc = 1;
+                job.err = sink.err.empty() ? std::string("reconstruction: ") + icon_last_error() : sink.err;
+                return;
+            }
+            r0 = r1;
         }
     }
     if (A.skip_cv) return;
@@ -175,7 +237,8 @@ void run_job(Job &job, const Args &A, const MrcHeader &inh, const std::vector<fl
     icon_geometry g{nx, thickness, nz - 1, t2.data(), cap, job.device};
     icon_plan *plan = nullptr;
     if (icon_plan_create(&g, &plan) != ICON_OK) return fail("cross-validation plan");
-    if (icon_plan_set_reprojection(plan, tilts[omit]) != ICON_OK) {
+    if (icon_plan_set_reprojection(plan, tilts[omit]) != ICON_OK || icon_plan_set_operator(plan, A.op) != ICON_OK ||
+        icon_plan_set_stop(plan, A.tol, 10) != ICON_OK) {
         icon_plan_destroy(plan);
         return fail("cross-validation reprojection angle");
     }
@@ -212,6 +275,10 @@ int main(int argc, char **argv)
             if (a == "--volume" && next_arg(argc, argv, i, v)) A.volume = v;
             else if (a == "--batch" && next_arg(argc, argv, i, v)) A.batch = std::max(1, atoi(v.c_str()));
             else if (a == "--loo") { A.loo = true; ++i; }
+            else if (a == "--resume") { A.resume = true; ++i; }
+            else if (a == "--tol" && next_arg(argc, argv, i, v)) A.tol = std::max(0.0, atof(v.c_str()));
+            else if (a == "--operator" && next_arg(argc, argv, i, v) && (v == "nufft" || v == "toeplitz"))
+                A.op = v == "toeplitz" ? ICON_OPERATOR_TOEPLITZ : ICON_OPERATOR_NUFFT;
             else if (a == "--help") { help(); return -1; }
             else { printf("parameter error!\n Please use -help to see the manual\n"); return -1; }
             continue;

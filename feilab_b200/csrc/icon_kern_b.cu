@@ -73,6 +73,62 @@ void Launch<B>::ypass_toep_quad(int E, dim3 grid, int threads, size_t smem, cuda
     else k_ypass_toep_quad<B, 16><<<grid, threads, smem, st>>>(g, G1, part);
 }
 
+// k_xtoep for one (BH, NA, NB) shape: grid (N1 * B/BH, G), half-groups fastest.
+template <int B, int BH, int LA, int LNB>
+static void xt_go(int mode, cudaStream_t st, int G, const XtArgs &a)
+{
+    using S = XtShape<BH, LA, LNB>;
+    const dim3 grid((unsigned)(a.N1 * (B / BH)), (unsigned)G);
+    const size_t smem = xtoep_smem(S::N, BH);
+    if (mode == 0) k_xtoep<B, BH, LA, LNB, 0><<<grid, S::T, smem, st>>>(a);
+    else k_xtoep<B, BH, LA, LNB, 1><<<grid, S::T, smem, st>>>(a);
+}
+template <int B, int BH, int LA, int LNB>
+static cudaError_t xt_attr()
+{
+    const int bytes = (int)xtoep_smem(XtShape<BH, LA, LNB>::N, BH);
+    cudaError_t e = cudaFuncSetAttribute((const void *)k_xtoep<B, BH, LA, LNB, 0>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute((const void *)k_xtoep<B, BH, LA, LNB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                bytes);
+}
+
+// Slices per CTA: all B up to n0 = 1024, then at most 8192 / n0 (a CTA's
+// transposed values stay at 64 KB, two CTAs per SM).
+#define ICON_XT_SHAPES(X)                            \
+    X(128, B, 2, 0)                                   \
+    X(256, B, 3, 0)                                   \
+    X(512, B, 4, 0)                                   \
+    X(1024, B, 5, 0)                                  \
+    X(2048, (B < 4 ? B : 4), 3, 3)                    \
+    X(4096, (B < 2 ? B : 2), 4, 3)                    \
+    X(8192, 1, 4, 4)
+
+template <int B>
+bool Launch<B>::xtoep(int mode, cudaStream_t st, int G, const XtArgs &a)
+{
+    switch (a.n0) {
+#define X(N, BH, LA, LNB) \
+    case N: xt_go<B, BH, LA, LNB>(mode, st, G, a); return true;
+        ICON_XT_SHAPES(X)
+#undef X
+    default: return false;
+    }
+}
+
+template <int B>
+cudaError_t Launch<B>::xtoep_prepare(int n0)
+{
+    switch (n0) {
+#define X(N, BH, LA, LNB) \
+    case N: return xt_attr<B, BH, LA, LNB>();
+        ICON_XT_SHAPES(X)
+#undef X
+    default: return cudaSuccess;
+    }
+}
+
 template <int B>
 void Launch<B>::ypass_fwd(int E, bool herm, dim3 grid, int threads, size_t smem, cudaStream_t st, const Geo &g,
                           const float2 *G1, float2 *P)

@@ -1408,3 +1408,354 @@ __host__ __device__ inline size_t ytoep4_smem(int n1, int B) { return (size_t)n1
 __host__ __device__ inline bool ytoep4_fits(int n1) { return n1 >= 128 && n1 <= 1024; }
 
 }  // namespace icon
+
+namespace icon {
+
+// ------------------------------------------- Toeplitz x-passes, 3-step ----
+// The x-direction transforms of the Toeplitz iteration, n0 = 32 NA NB
+// (NA = 2^LA, NB = 2^LNB), as a register-resident three-step FFT over the
+// BH slices (of a B-slice group) that one CTA takes.  With
+// x = 32 NB a + 32 b + c (a < NA, b < NB, c < 32) and
+// k = ka + NA kb + NA NB kc:
+//   X[k] = sum_c w32^(c kc) wn^(NA c kb) sum_b wNB^(b kb) wn^((32 b + c) ka)
+//          sum_a wNA^(a ka) x[32 NB a + 32 b + c].
+// Thread u (of U = NA NB per slice) does the NA-point DFTs over a of the
+// columns tau = 32 b + c = u + U i (i < 32 / NA), then, after a transpose,
+// the NB-point DFTs over b of (ka, c) = (tau >> 5, tau & 31) for
+// tau = u + U i (i < 32 / NB), then, after a second transpose, the 32-point
+// DFT over c of (ka, kb) = (u mod NA, u / NA): it ends holding frequencies
+// u + U kc, which go straight to rows u + U kc of G1.  The inverse reads those
+// rows into the same registers and runs the steps backwards, ending with the
+// values of x = 32 NB a + tau for its columns tau: the columns its forward
+// step 1 starts from.  So the adjoint x-pass (crop, r-hat = . - Ahwb, |r-hat|^2)
+// and the forward x-pass of r-hat fuse into one kernel whose r-hat never
+// leaves registers between the two transforms, and the update
+// m <- m - alpha Re r-hat (with the clamp) fuses into the forward x-pass of m.
+// Inputs and outputs are read and written straight from and to global memory
+// (a warp covers consecutive x, i.e. 32/BH points of BH x 8 bytes); the two
+// transposes go through one shared buffer, [ka][tau][BH] after step 1 and
+// [ka][kb][c][BH] after step 2, with the innermost index XOR-swizzled by the
+// low bits of ka where a warp's lanes differ in ka, so that every access
+// takes the minimum two wavefronts.  Each slice stays its own transform.
+struct XtArgs {
+    int N0, N1, n0;
+    const float2 *tw0;       // [n0] exp(-2 pi i q / n0)
+    float2 *G1;              // [G][n0][N1][B]
+    float *m;                // [G][N1][N0][B] real image (forward input; updated in place when upd)
+    const float2 *rhat_in;   // update: r-hat of the iteration being finished
+    const double *alpha;     // update: [G*B] step lengths
+    int upd, clamp, data_type;
+    float thr;
+    float2 *rhat;            // mid: r-hat out, [G][N1][N0][B]
+    const float2 *Ahwb;      // mid: [G][N1][N0][B]
+    double *part_rtr;        // mid: [G][N1][B] partial |r-hat|^2 per column
+};
+
+template <int BH, int LA, int LNB>
+struct XtShape {
+    static constexpr int NA = 1 << LA, NB = 1 << LNB, U = NA * NB, T = U * BH;
+    static constexpr int N = 32 * U;
+    static constexpr int NI1 = 32 / NA, NI2 = 32 / NB;
+    static constexpr int SW = 16 / BH - 1;
+    // unit (float2) index of (ka, tau, s) after step 1 and of (ka, kb, c, s)
+    // after step 2
+    __device__ static __forceinline__ int e1(int ka, int tau, int s)
+    {
+        const int t = (NB == 1) ? (tau ^ (ka & SW)) : tau;
+        return (ka * 32 * NB + t) * BH + s;
+    }
+    __device__ static __forceinline__ int e2(int ka, int kb, int c, int s)
+    {
+        return ((ka * NB + kb) * 32 + (c ^ (ka & SW))) * BH + s;
+    }
+};
+
+// x^(e) times wn^(base*j) for j = 1..R-1 in place, the twiddles formed from
+// the table at multiples of 8 and by products in between; CONJ: conjugates.
+template <int R, bool CONJ>
+__device__ __forceinline__ void xt_twiddle(float2 (&v)[R], const float2 *__restrict__ tw, int base)
+{
+    float2 w1 = __ldg(&tw[base]);
+    if (CONJ) w1.y = -w1.y;
+    float2 t = w1;
+#pragma unroll
+    for (int j = 1; j < R; ++j) {
+        if ((j & 7) == 0) {
+            t = __ldg(&tw[base * j]);
+            if (CONJ) t.y = -t.y;
+        } else if (j > 1) {
+            t = cmul(t, w1);
+        }
+        v[j] = cmul(v[j], t);
+    }
+}
+
+// Forward transform from the step-1 registers v[i][a] (input at
+// x = 32 NB a + u + U i) to G1 rows u + U kc of column `col` (pointer to
+// row 0 of the column for this thread's slice; rows N1*B float2 apart).
+template <int BH, int LA, int LNB>
+__device__ __forceinline__ void xt_forward(float2 (&v)[32 >> LA][1 << LA], float2 *s, int u, int sl,
+                                           const float2 *__restrict__ tw, float2 *col, size_t rstride)
+{
+    using S = XtShape<BH, LA, LNB>;
+    constexpr int NA = S::NA, NB = S::NB, U = S::U;
+#pragma unroll
+    for (int i = 0; i < S::NI1; ++i) {
+        const int tau = u + U * i;
+        float2 a[NA];
+#pragma unroll
+        for (int j = 0; j < NA; ++j) a[brev5(j) >> (5 - LA)] = v[i][j];
+        dft_inplace<NA>(a, -1.f);
+        if (tau) xt_twiddle<NA, false>(a, tw, tau);
+#pragma unroll
+        for (int ka = 0; ka < NA; ++ka) s[S::e1(ka, tau, sl)] = a[ka];
+    }
+    __syncthreads();
+    if constexpr (NB > 1) {
+        float2 v2[S::NI2][NB];
+#pragma unroll
+        for (int i = 0; i < S::NI2; ++i) {
+            const int t2 = u + U * i, c = t2 & 31, ka = t2 >> 5;
+#pragma unroll
+            for (int b = 0; b < NB; ++b) v2[i][brev5(b) >> (5 - LNB)] = s[S::e1(ka, 32 * b + c, sl)];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < S::NI2; ++i) {
+            const int t2 = u + U * i, c = t2 & 31, ka = t2 >> 5;
+            dft_inplace<NB>(v2[i], -1.f);
+            if (c) xt_twiddle<NB, false>(v2[i], tw, NA * c);
+#pragma unroll
+            for (int kb = 0; kb < NB; ++kb) s[S::e2(ka, kb, c, sl)] = v2[i][kb];
+        }
+        __syncthreads();
+    }
+    float2 w[32];
+    {
+        const int ka = u % NA, kb = u / NA;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) w[brev5(c)] = (NB > 1) ? s[S::e2(ka, kb, c, sl)] : s[S::e1(ka, c, sl)];
+    }
+    dft_inplace<32>(w, -1.f);
+    float2 *p = col + (size_t)u * rstride;
+    const size_t step = (size_t)U * rstride;
+#pragma unroll
+    for (int kc = 0; kc < 32; ++kc, p += step) *p = w[kc];
+}
+
+// Inverse transform from the column staged in s ([x][BH], rows u + U kc
+// of this thread's slice) to the step-1 registers v[i][a] (value at
+// x = 32 NB a + u + U i).  Ends after a barrier-free last step: the caller
+// syncs before writing s again.
+template <int BH, int LA, int LNB>
+__device__ __forceinline__ void xt_inverse(float2 (&v)[32 >> LA][1 << LA], float2 *s, int u, int sl,
+                                           const float2 *__restrict__ tw)
+{
+    using S = XtShape<BH, LA, LNB>;
+    constexpr int NA = S::NA, NB = S::NB, U = S::U;
+    {
+        // The column, staged in s as [x][BH]: rows u + U kc of this slice.
+        float2 w[32];
+#pragma unroll
+        for (int kc = 0; kc < 32; ++kc) w[kc] = s[(u + U * kc) * BH + sl];
+        __syncthreads();                              // the staged column is consumed before s is rewritten
+        dft_dif_inplace<32>(w, +1.f);                 // Z[c] at w[brev5(c)]
+        const int ka = u % NA, kb = u / NA;
+        if constexpr (NB > 1) {
+            if (kb) {
+                float2 z[32];
+#pragma unroll
+                for (int c = 0; c < 32; ++c) z[c] = w[brev5(c)];
+                xt_twiddle<32, true>(z, tw, NA * kb);
+#pragma unroll
+                for (int c = 0; c < 32; ++c) w[brev5(c)] = z[c];
+            }
+#pragma unroll
+            for (int c = 0; c < 32; ++c) s[S::e2(ka, kb, c, sl)] = w[brev5(c)];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 32; ++c) s[S::e1(ka, c, sl)] = w[brev5(c)];
+        }
+    }
+    __syncthreads();
+    if constexpr (NB > 1) {
+        float2 v2[S::NI2][NB];
+#pragma unroll
+        for (int i = 0; i < S::NI2; ++i) {
+            const int t2 = u + U * i, c = t2 & 31, ka = t2 >> 5;
+#pragma unroll
+            for (int kb = 0; kb < NB; ++kb) v2[i][kb] = s[S::e2(ka, kb, c, sl)];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < S::NI2; ++i) {
+            const int t2 = u + U * i, c = t2 & 31, ka = t2 >> 5;
+            dft_dif_inplace<NB>(v2[i], +1.f);          // Z[b] at v2[brev(b)]
+#pragma unroll
+            for (int b = 0; b < NB; ++b) s[S::e1(ka, 32 * b + c, sl)] = v2[i][brev5(b) >> (5 - LNB)];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < S::NI1; ++i) {
+        const int tau = u + U * i;
+        float2 a[NA];
+#pragma unroll
+        for (int ka = 0; ka < NA; ++ka) a[ka] = s[S::e1(ka, tau, sl)];
+        if (tau) xt_twiddle<NA, true>(a, tw, tau);
+        dft_dif_inplace<NA>(a, +1.f);                  // x at a[brev(a)]
+#pragma unroll
+        for (int j = 0; j < NA; ++j) v[i][j] = a[brev5(j) >> (5 - LA)];
+    }
+}
+
+// MODE 0: G1 <- F_x(pad m) for every row, m first updated (upd: m <- m -
+// alpha Re r-hat_in, clamped on ICON steps, as k_update).  MODE 1: r-hat =
+// crop F_x^-1(G1) - Ahwb (stored, |r-hat|^2 partial sums per column), then
+// G1 <- F_x(pad r-hat) in place.  Grid: (N1 * B/BH, G), half-group fastest.
+template <int B, int BH, int LA, int LNB, int MODE>
+__global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>::T >= 256) ? 2 : 4)
+    k_xtoep(XtArgs g)
+{
+    using S = XtShape<BH, LA, LNB>;
+    constexpr int NA = S::NA, NB = S::NB, U = S::U, H = B / BH;
+    extern __shared__ float2 s[];
+    double *red = reinterpret_cast<double *>(s + S::N * BH);
+    const int Y = blockIdx.x / H, h = blockIdx.x % H, grp = blockIdx.y;
+    const int t = threadIdx.x, sl = t % BH, u = t / BH, bsl = h * BH + sl;   // bsl: slice within the group
+    const int N0 = g.N0, N1 = g.N1, n = S::N, half = N0 / 2;
+    const size_t rstride = (size_t)N1 * B;
+    float2 *col = g.G1 + ((size_t)grp * n * N1 + Y) * B + bsl;       // row x at col[x * rstride]
+    const size_t ibase = ((size_t)grp * N1 + Y) * N0 * B + bsl;        // image point X at ibase + X*B
+    float2 v[S::NI1][NA];
+    float2 *As = s + S::N * BH + S::T;   // mid: this CTA's Ahwb column, [N0][BH]
+    if constexpr (MODE == 1) {
+        // The G1 column (n0 rows of BH values, rows N1*B float2 apart) into s
+        // as [x][BH], then the Ahwb column, staged while the inverse runs.
+        const float2 *gsrc = g.G1 + ((size_t)grp * n * N1 + Y) * B + h * BH;
+        if constexpr (BH >= 2) {
+            constexpr int P = BH / 2;
+            for (int idx = t; idx < n * P; idx += S::T) {
+                const int x = idx / P, c = idx - x * P;
+                cp_async<16>(s + x * BH + 2 * c, gsrc + (size_t)x * rstride + 2 * c);
+            }
+        } else {
+            for (int x = t; x < n; x += S::T) cp_async<8>(s + x, gsrc + (size_t)x * rstride);
+        }
+        cp_async_commit();
+        const float2 *src = g.Ahwb + ((size_t)grp * N1 + Y) * N0 * B + h * BH;
+        if constexpr (BH >= 2) {
+            constexpr int P = BH / 2;                     // 16-byte pieces per point
+            for (int idx = t; idx < N0 * P; idx += S::T) {
+                const int X = idx / P, c = idx - X * P;
+                cp_async<16>(As + X * BH + 2 * c, src + (size_t)X * B + 2 * c);
+            }
+        } else {
+            for (int X = t; X < N0; X += S::T) cp_async<8>(As + X, src + (size_t)X * B);
+        }
+        cp_async_commit();
+    }
+    if constexpr (MODE == 0) {
+        // The m column (N0 x BH floats) into s and, for the update, the r-hat
+        // column into As, by cp.async; then into registers.
+        float *Ms = reinterpret_cast<float *>(s);
+        {
+            const float *msrc = g.m + ibase - sl;           // point X of this CTA's slices at msrc + X*B
+            const float2 *rsrc = g.rhat_in + ibase - sl;
+            for (int X = t; X < N0; X += S::T) {
+                if constexpr (BH == 4) cp_async<16>(Ms + X * 4, msrc + (size_t)X * B);
+                else if constexpr (BH == 2) cp_async<8>(Ms + X * 2, msrc + (size_t)X * B);
+                else if constexpr (BH == 1) cp_async<4>(Ms + X, msrc + (size_t)X * B);
+                else {
+                    cp_async<16>(Ms + X * BH, msrc + (size_t)X * B);
+                    cp_async<16>(Ms + X * BH + 4, msrc + (size_t)X * B + 4);
+                }
+            }
+            if (g.upd) {
+                constexpr int P = BH >= 2 ? BH / 2 : 1;
+                for (int idx = t; idx < N0 * P; idx += S::T) {
+                    const int X = idx / P, c = idx - X * P;
+                    if constexpr (BH >= 2) cp_async<16>(As + X * BH + 2 * c, rsrc + (size_t)X * B + 2 * c);
+                    else cp_async<8>(As + X, rsrc + (size_t)X * B);
+                }
+            }
+            cp_async_commit();
+            cp_async_wait<0>();
+            __syncthreads();
+        }
+        if (g.upd) {
+            // m <- m - alpha Re r-hat (k_update's arithmetic), clamped on ICON
+            // steps, over the staged column by all threads (coalesced stores).
+            float *mdst = g.m + ibase - sl;
+            for (int idx = t; idx < N0 * BH; idx += S::T) {
+                const int X = idx / BH, q = idx - X * BH;
+                const double al = g.alpha[grp * B + h * BH + q];
+                float nv = (float)((double)Ms[idx] - al * (double)As[idx].x);
+                if (g.clamp) {
+                    if (g.data_type == 1) {
+                        if (nv > g.thr) nv = g.thr;
+                    } else {
+                        if (nv < g.thr) nv = g.thr;
+                    }
+                }
+                Ms[idx] = nv;
+                mdst[(size_t)X * B + q] = nv;
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int i = 0; i < S::NI1; ++i) {
+            const int tau = u + U * i;
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+                const int X = (32 * NB * a + tau + half) & (n - 1);
+                v[i][a] = make_float2(X < N0 ? Ms[X * BH + sl] : 0.f, 0.f);
+            }
+        }
+        __syncthreads();   // the staged m is read before step 1 rewrites s
+        xt_forward<BH, LA, LNB>(v, s, u, sl, g.tw0, col, rstride);
+    } else {
+        cp_async_wait<1>();    // the column group (Ahwb may still be landing)
+        __syncthreads();
+        xt_inverse<BH, LA, LNB>(v, s, u, sl, g.tw0);
+        cp_async_wait<0>();
+        __syncthreads();   // Ahwb staged; every read of s by the inverse is done
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < S::NI1; ++i) {
+            const int tau = u + U * i;
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+                const int x = 32 * NB * a + tau;
+                const int X = (x + half) & (n - 1);
+                float2 r = make_float2(0.f, 0.f);
+                if (X < N0) {
+                    const float2 av = As[X * BH + sl];
+                    r = make_float2(v[i][a].x - av.x, v[i][a].y - av.y);
+                    acc += (double)r.x * (double)r.x + (double)r.y * (double)r.y;
+                    g.rhat[ibase + (size_t)X * B] = r;
+                }
+                v[i][a] = r;
+            }
+        }
+        xt_forward<BH, LA, LNB>(v, s, u, sl, g.tw0, col, rstride);
+        // per-slice FP64 sum in a fixed order (thread t holds slice t % BH)
+        red[t] = acc;
+        __syncthreads();
+        for (int stride = S::T >> 1; stride >= BH; stride >>= 1) {
+            if (t < stride) red[t] += red[t + stride];
+            __syncthreads();
+        }
+        if (t < BH) g.part_rtr[((size_t)grp * N1 + Y) * B + h * BH + t] = red[t];
+    }
+}
+
+// Shared memory of k_xtoep: the transposed values, the reduction scratch
+// and (mid) the staged Ahwb column of N0 <= n0 / 2 points.
+__host__ __device__ inline size_t xtoep_smem(int n0, int BH)
+{
+    return (size_t)n0 * BH * sizeof(float2) + (size_t)(n0 * BH / 32) * sizeof(double) +
+           (size_t)(n0 / 2) * BH * sizeof(float2);
+}
+
+}  // namespace icon

@@ -8,6 +8,7 @@ namespace icon {
 
 struct Geo;
 struct Geo1;
+struct XtArgs;
 
 template <int B>
 struct Launch {
@@ -37,6 +38,13 @@ struct Launch {
                         const float2 *f, float *out, int S);
     static void update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat, const double *alpha, int per_group,
                        int clamp, int data_type, float thr, double *step_part = nullptr);
+    // Toeplitz x-passes (k_xtoep) over G groups: mode 0 the forward of the
+    // real image (with the fused update when a.upd), mode 1 the inverse, r-hat
+    // and the forward of r-hat.  Returns false when n0 has no variant (the
+    // caller then uses the Stockham x-passes).
+    static bool xtoep(int mode, cudaStream_t st, int G, const XtArgs &a);
+    // Raises the shared-memory limit of the k_xtoep variants for n0.
+    static cudaError_t xtoep_prepare(int n0);
     // Raises the dynamic shared-memory limit of every kernel variant a plan uses.
     static cudaError_t set_smem(int ex, int ey, size_t smem_x, size_t need_x, size_t smem_y, size_t smem_ya,
                                 size_t smem_yt);

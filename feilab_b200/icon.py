@@ -57,6 +57,7 @@ def lib():
         L.icon_weights.argtypes = [I, I, V, V]
         L.icon_plan_set_group_weights.argtypes = [P, V, I]
         L.icon_plan_set_operator.argtypes = [P, I]
+        L.icon_plan_set_stop.argtypes = [P, ctypes.c_double, I]
         L.icon_trace_enable.argtypes = [P, I]
         L.icon_trace_read.argtypes = [P, V, V, V]
         L.icon_launch_count.argtypes = [P]
@@ -68,7 +69,7 @@ def lib():
                      "icon_reconstruct_host", "icon_trace_enable", "icon_trace_read", "icon_prepare_rhs_stack",
                      "icon_reconstruct_stack", "icon_reconstruct_stack_host", "icon_host_alloc", "icon_host_free",
                      "icon_stack_upload", "icon_device_free", "icon_weights", "icon_plan_set_group_weights",
-                     "icon_plan_set_operator"):
+                     "icon_plan_set_operator", "icon_plan_set_stop"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -153,6 +154,12 @@ class IconPlan:
         kernel of the node set; see icon_plan_set_operator)."""
         _check(lib().icon_plan_set_operator(self._h, self.OPERATORS[op]))
         self.operator = op
+
+    def set_stop(self, tol=0.0, check_every=10):
+        """Tolerance stop of the reconstruct calls (icon_plan_set_stop): their
+        ICON phase ends once every slice's relative step is within tol;
+        tol = 0 runs the whole schedule."""
+        _check(lib().icon_plan_set_stop(self._h, float(tol), int(check_every)))
 
     def geometry(self):
         xy = np.zeros((self.M, 2), np.float32)
@@ -341,7 +348,7 @@ class IconPlan:
                                                  int(S), int(outputs), cb, None, _stream()))
 
     TRACE_KINDS = ("xpass_fwd", "ypass_fwd", "interp_fin", "ypass_adj", "xpass_adj", "alpha", "update", "rows_fwd",
-                   "layout", "row_adj", "ypass_toep", "ypass_toep_quad")
+                   "layout", "row_adj", "ypass_toep", "ypass_toep_quad", "xtoep_fwd", "xtoep_mid")
 
     def trace(self, enable=True):
         _check(lib().icon_trace_enable(self._h, int(bool(enable))))

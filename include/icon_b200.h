@@ -133,6 +133,15 @@ icon_status icon_plan_set_group_weights(icon_plan *plan, const float *h_w, int n
 #define ICON_OPERATOR_TOEPLITZ 1
 icon_status icon_plan_set_operator(icon_plan *plan, int op);
 
+/* Tolerance stop of the reconstruct calls (icon_reconstruct_host,
+ * icon_reconstruct_stack, icon_reconstruct_stack_host): with tol > 0 their
+ * ICON phase ends, per batch, once every slice's relative step
+ * ||m_new - m_old|| / ||m_new|| is at or below tol, checked every
+ * check_every ICON iterations, as icon_solve_until does; tol = 0 (the
+ * default) runs the whole schedule, as the reference always does
+ * (Iteration2.cu:42-146).  No counterpart in the reference. */
+icon_status icon_plan_set_stop(icon_plan *plan, double tol, int check_every);
+
 /* Forward 2-D NUFFT of real images: d_nodes = A d_img.
  * Replaces cunfft_trafo_2d_R2C2 (NU:984-1076). */
 icon_status icon_nufft_forward(icon_plan *plan, const float *d_img, void *d_nodes, int S, void *stream);
@@ -237,6 +246,13 @@ icon_status icon_solve_until(icon_plan *plan, const icon_solve_cfg *cfg, const v
  * cunfft_adjoint_1d NU:1518-1536).  d_out[S][nx]. */
 icon_status icon_reproject(icon_plan *plan, const float *d_m, float tilt_deg, float *d_out, int S, void *stream);
 
+/* icon_reproject from and to host memory: h_m [S][N0][N1] (Y fastest),
+ * h_out [S][nx]; S may exceed the capacity (processed in chunks through the
+ * plan's buffers).  Returns when h_out is filled.  Used by icon-gpu --resume
+ * for slices whose files a previous run wrote (the reference recomputes
+ * every slice, MainCode.cu:113-162). */
+icon_status icon_reproject_host(icon_plan *plan, const float *h_m, float tilt_deg, float *h_out, int S, void *stream);
+
 /* The whole per-slice pipeline of Lib_2D2 (MainCode.cu:113-142) for S
  * slices from host memory: rows in, reconstructed slices out, plus the
  * reprojection when h_reproj is not NULL -- at the smallest-|angle| tilt of
@@ -256,8 +272,11 @@ icon_status icon_reconstruct_host(icon_plan *plan, const icon_solve_cfg *cfg, co
  * kinds returns the number of launches, their summed device time in ms and,
  * when h_bytes is not NULL, their summed algorithmic bytes (the data each
  * launch must read and write at least once), then clears the record.  Kinds, in order: xpass_fwd, ypass_fwd, interp_fin,
- * ypass_adj, xpass_adj, alpha, update, rows_fwd, layout, row_adj, ypass_toep, ypass_toep_quad. */
-#define ICON_TRACE_KERNELS 12
+ * ypass_adj, xpass_adj, alpha, update, rows_fwd, layout, row_adj, ypass_toep, ypass_toep_quad,
+ * xtoep_fwd (the Toeplitz forward x-pass of m, with the previous iteration's
+ * update), xtoep_mid (the Toeplitz inverse x-pass, r-hat and forward x-pass
+ * of r-hat in one kernel). */
+#define ICON_TRACE_KERNELS 14
 icon_status icon_trace_enable(icon_plan *plan, int enable);
 icon_status icon_trace_read(icon_plan *plan, int *h_count, double *h_ms, double *h_bytes);
 

@@ -140,3 +140,71 @@ def test_cli_leave_one_out(golden, tmp_path):
     assert summary.shape == (nz, 4)
     np.testing.assert_allclose(summary[:, 1], z["tilts"], atol=1e-5)
     assert np.all(summary[:, 3] == a + b + c)
+
+
+def _cli_case(golden, tmp_path, name="res", sched=None):
+    from feilab_b200 import mrc
+    z = golden["cli"]
+    stack, tlt, out = tmp_path / "stack.mrc", tmp_path / "cli.tlt", tmp_path / name
+    if not stack.exists():
+        mrc.write_tilt_series(str(stack), z["rows"])
+        mrc.write_tlt(str(tlt), z["tilts"])
+    out.mkdir()
+    a, b, c = sched or (int(v) for v in z["sched"])
+    base = ["-i", str(stack), "-t", str(tlt), "-o", str(out), "-s", f"0,{int(z['S']) - 1}", "-iter", f"{a},{b},{c}",
+            "-d", str(int(z["data_type"])), "-thr", str(float(z["threshold"])), "-g", "0", "-thi",
+            str(int(z["thickness"]))]
+    return z, out, base
+
+
+@pytest.mark.gpu
+def test_cli_resume_keeps_finished_slices(golden, tmp_path):
+    # A run whose slice files are partly there (an interrupted run) resumed
+    # with --resume: the missing slices are reconstructed, the others read
+    # back; every output file equals an uninterrupted run's byte for byte
+    # (the reprojections of the read-back slices are recomputed from them).
+    z, out, base = _cli_case(golden, tmp_path)
+    S = int(z["S"])
+    p = _run(base, str(tmp_path))
+    assert p.returncode == 0, p.stdout + p.stderr
+    first = {f: (out / f).read_bytes() for f in
+             [f"reconstruction/mid{s:05d}.mrc" for s in range(S)] +
+             [f"crossValidation/{n}" for n in ("fullRec_reProjection.mrc", "crossV_reprojection.mrc", "fullRec.frc",
+                                               "crossV.frc")]}
+    (out / "reconstruction" / "mid00001.mrc").unlink()
+    (out / "reconstruction" / f"mid{S - 1:05d}.mrc").write_bytes(b"truncated")
+    for n in ("fullRec_reProjection.mrc", "crossV_reprojection.mrc", "fullRec.frc", "crossV.frc"):
+        (out / "crossValidation" / n).unlink()
+    p = _run(base + ["--resume"], str(tmp_path))
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert f"resume: {S - 2} of {S} slices" in p.stdout
+    assert "slice 1 finished" in p.stdout and "slice 0 finished" not in p.stdout
+    for f, data in first.items():
+        assert (out / f).read_bytes() == data, f
+
+
+@pytest.mark.gpu
+def test_cli_toeplitz_operator_and_tolerance(golden, tmp_path):
+    # --operator toeplitz reconstructs within the parity bar of the default
+    # (NUFFT) run; --tol with a loose tolerance stops the ICON phase early
+    # (slices differ, but stay close).
+    from feilab_b200 import mrc
+    sched = (1, 40, 1)
+    z, out, base = _cli_case(golden, tmp_path, "nufft", sched)
+    S, th, nx = int(z["S"]), int(z["thickness"]), int(z["nx"])
+    assert _run(base + ["-skipCV", "1"], str(tmp_path)).returncode == 0
+    zt, out_t, base_t = _cli_case(golden, tmp_path, "toep", sched)
+    p = _run(base_t + ["-skipCV", "1", "--operator", "toeplitz"], str(tmp_path))
+    assert p.returncode == 0, p.stdout + p.stderr
+    _, out_l, base_l = _cli_case(golden, tmp_path, "tol", sched)
+    p = _run(base_l + ["-skipCV", "1", "--tol", "0.5"], str(tmp_path))
+    assert p.returncode == 0, p.stdout + p.stderr
+    for s in range(S):
+        _, d = mrc.read(str(out / "reconstruction" / f"mid{s:05d}.mrc"))
+        _, dt = mrc.read(str(out_t / "reconstruction" / f"mid{s:05d}.mrc"))
+        _, dl = mrc.read(str(out_l / "reconstruction" / f"mid{s:05d}.mrc"))
+        assert d.shape == dt.shape == dl.shape == (1, th, nx)
+        assert rel_l2(dt[0], d[0]) < TOL_SOLVE, s
+        assert 0 < rel_l2(dl[0], d[0]) < 0.5, s
+    p = _run(base + ["-skipCV", "1", "--operator", "other"], str(tmp_path))
+    assert p.returncode != 0 and "parameter error!" in p.stdout

@@ -163,7 +163,7 @@ def test_toeplitz_iteration_matches_nufft_iteration_at_large_shapes(nx, th, ntil
     # y-transform lengths that the fixtures above do not reach.
     from feilab_b200 import icon
     tilts = np.linspace(-60, 60, ntilt).astype(np.float32)
-    p = icon.IconPlan(nx, th, tilts, capacity=4)
+    p = icon.IconPlan(nx, th, tilts, capacity=8)
     rng = np.random.default_rng(nx + th)
     S = 3
     m0 = rng.standard_normal((S, nx, th)).astype(np.float32)
