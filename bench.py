@@ -469,6 +469,8 @@ def run_ours(args):
     if rank == 0:
         line["parity"] = {op: parity_leg(lambda n: icon.IconPlan(NX, THICK, tilts, capacity=n, device=local), op)
                           for op in ops}
+    if rank == 0 and world == 1 and args.uneven_scale > 0:
+        line["uneven_batch"] = uneven_leg(args, args.uneven_scale)
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_leg(tilts, rows[0], plan)
         if "value" in line["reference_gpu"]:
@@ -537,6 +539,68 @@ def warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S):
             "weights": f"feilab_b200/weights/warmstart_{NX}x{THICK}.npz (trained on {meta.get('train_slices')} slices)"}
 
 
+TUNE_CACHE = os.path.join(ROOT, "feilab_b200", "tune", "b200_uneven.txt")
+
+
+def uneven_leg(args, slice_scale):
+    """The uneven multi-series workload (24 seeded series: widths 256-2048,
+    64-512 slices times slice_scale, thickness 100-400, tilt ranges +-45..70
+    with 10% of the tilts dropped, SNR 0.1-0.5; the full schedule 10,280,10)
+    through icon_batch: all series at once from CUDA graphs with the tuned
+    slices per group and per launch (tuning from the committed cache file,
+    shapes missing from it timed here), against the same series one after
+    another (same plans, direct launches).  Wall time around the host call,
+    pinned rows in and slices out, so copies are inside."""
+    import torch
+    from feilab_b200 import icon, synth
+    t0 = time.perf_counter()
+    ser = synth.uneven_batch(24, seed=3003, slice_scale=slice_scale, device="cuda")
+    gen_s = time.perf_counter() - t0
+    shapes = [(d["nx"], d["thickness"], d["tilts"], d["slices"]) for d in ser]
+    rows = [d["rows"].cpu().pin_memory() for d in ser]
+    del ser
+    torch.cuda.empty_cache()
+    if args.tune_write:
+        cache, tune = args.tune_write, 2
+    else:
+        cache, tune = (TUNE_CACHE if os.path.exists(TUNE_CACHE) else None), 1
+    t0 = time.perf_counter()
+    b = icon.IconBatch(shapes, operator="toeplitz", tune_cache=cache, tune=tune)
+    setup_s = time.perf_counter() - t0
+    out = [torch.empty((sl, nx, th), dtype=torch.float32, pin_memory=True) for nx, th, _, sl in shapes]
+    total = sum(sl for *_, sl in shapes)
+    res = {}
+    for mode, conc in (("concurrent_graphs", True), ("one_series_at_a_time", False)):
+        # warm-up: every graph kind of the schedule captured, every chunk size met
+        b.reconstruct(rows, (2, 2, 2), DATA_TYPE, THRESHOLD, out=out, concurrent=conc)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.reconstruct(rows, SCHED, DATA_TYPE, THRESHOLD, out=out, concurrent=conc)
+        t = time.perf_counter() - t0
+        res[mode] = {"value": total / t, "unit": "slices/s", "seconds": round(t, 3)}
+    tun = [b.tuning(k) for k in range(len(shapes))]
+    b.close()
+    # The same concurrent run with the built-in defaults (8 slices per group
+    # where the size allows, 128 slices per launch): what the tuning gains.
+    b = icon.IconBatch(shapes, operator="toeplitz", tune_cache=None, tune=0)
+    b.reconstruct(rows, (2, 2, 2), DATA_TYPE, THRESHOLD, out=out, concurrent=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.reconstruct(rows, SCHED, DATA_TYPE, THRESHOLD, out=out, concurrent=True)
+    t = time.perf_counter() - t0
+    res["concurrent_default_tuning"] = {"value": total / t, "unit": "slices/s", "seconds": round(t, 3)}
+    b.close()
+    return {"workload": f"24 seeded series, slice_scale {slice_scale}", "slices": total,
+            "series": [{"nx": nx, "thickness": th, "tilts": len(t), "slices": sl, "group": tu["group"],
+                        "chunk": tu["chunk"], "tuned": tu["tuned"]} for (nx, th, t, sl), tu in zip(shapes, tun)],
+            **res, "speedup_concurrent": round(res["concurrent_graphs"]["value"] /
+                                               res["one_series_at_a_time"]["value"], 3),
+            "speedup_tuning": round(res["concurrent_graphs"]["value"] /
+                                    res["concurrent_default_tuning"]["value"], 3),
+            "setup_s": round(setup_s, 2), "generate_s": round(gen_s, 2),
+            "iterations": sum(SCHED), "operator": "toeplitz"}
+
+
 def run_profile_case(args):
     """Small case for ncu captures: --profile-slices slices of the workload
     (32 by default: the grid intermediate of every kernel, 157 MB, is larger
@@ -569,11 +633,21 @@ def main():
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference ICON-GPU leg")
     ap.add_argument("--operator", default="toeplitz", choices=["nufft", "toeplitz"],
                     help="normal operator of the headline run (the other is timed beside it)")
+    ap.add_argument("--uneven-scale", type=float, default=0.25,
+                    help="slice-count scale of the 24-series uneven batch leg (0 skips it; 1 is the full workload)")
+    ap.add_argument("--uneven-only", action="store_true", help="run the uneven batch leg only and print it")
+    ap.add_argument("--tune-write", default=None,
+                    help="tuning cache file to read and extend (time every shape missing from it)")
     ap.add_argument("--profile", action="store_true", help="run the small ncu case only")
     ap.add_argument("--profile-slices", type=int, default=32, help="slices of the --profile case")
     args = ap.parse_args()
     if args.profile:
         run_profile_case(args)
+        return
+    if args.uneven_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"uneven_batch": uneven_leg(args, args.uneven_scale)}), flush=True)
         return
     if args.warmup < 3:
         args.warmup = 3

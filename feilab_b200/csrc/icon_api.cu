@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "icon_b200.h"
+#include "icon_internal.h"
 #include "icon_kernels.cuh"
 #include "icon_launch.h"
 
@@ -151,6 +152,16 @@ struct Arena {
         bufs.push_back(std::move(b));
         return ICON_OK;
     }
+    // Releases one buffer of this arena (reallocation of a grown table).
+    void release(void *ptr)
+    {
+        for (auto it = bufs.begin(); it != bufs.end(); ++it)
+            if ((*it)->p == ptr) {
+                total -= (*it)->bytes;
+                bufs.erase(it);
+                return;
+            }
+    }
     template <typename T>
     icon_status upload(T **out, const T *host, size_t count)
     {
@@ -201,6 +212,7 @@ struct icon_plan {
     int stop_every = 10;
     float *Kt = nullptr;        // [Gcap][n0][n1] Toeplitz kernels (one used unless per-group weights)
     int kt_groups = 0;          // kernels computed for: 1 = the plan's weights, Gcap = per-group weights
+    int kt_cap = 0;             // kernels the Kt table has room for
     bool kt_stale = true;
     float *ones0 = nullptr, *ones1 = nullptr;   // unit deapodisation of the Toeplitz x-passes
     size_t smem_yt = 0;
@@ -484,11 +496,18 @@ icon_status launch_adjoint(icon_plan *p, const float2 *f_int, int G, int mode, f
     const double slots = (double)G * p->B;
     dim3 gy(G, p->n0), gx(p->N1, G);
     size_t smem = p->smem_x + sizeof(double) * p->thr_x;
+    icon::XtArgs xa{};
+    xa.N0 = p->N0; xa.N1 = p->N1; xa.n0 = p->n0; xa.tw0 = p->tw0; xa.G1 = p->G1; xa.rhat = out_int;
+    xa.Ahwb = p->Ahwb; xa.part_rtr = p->part_rtr; xa.rcx = p->rcx; xa.rcy = p->rcy; xa.resid = mode == 0 ? 0 : 1;
     WITH_B(p->B,
         LAUNCH_B(p, K_YA, st, sb.ya * slots, L::ypass_adj(p->ey, gy, p->thr_y, p->smem_ya, st, g, f_int, p->G1));
-        LAUNCH_B(p, K_XA, st, (mode == 0 ? sb.xa_plain : sb.xa_resid) * slots,
-                 L::xpass_adj(mode, p->ex, gx, p->thr_x, smem, st, g, p->G1, out_int, mode == 0 ? nullptr : p->Ahwb,
-                              mode == 0 ? nullptr : p->part_rtr)))
+        if (p->xt_ok) {
+            LAUNCH_B(p, K_XA, st, (mode == 0 ? sb.xa_plain : sb.xa_resid) * slots, L::xtoep(2, st, G, xa));
+        } else {
+            LAUNCH_B(p, K_XA, st, (mode == 0 ? sb.xa_plain : sb.xa_resid) * slots,
+                     L::xpass_adj(mode, p->ex, gx, p->thr_x, smem, st, g, p->G1, out_int, mode == 0 ? nullptr : p->Ahwb,
+                                  mode == 0 ? nullptr : p->part_rtr));
+        })
     ICON_CUDA(cudaGetLastError());
     return ICON_OK;
 }
@@ -544,7 +563,14 @@ icon_status ensure_toeplitz(icon_plan *p, cudaStream_t st)
 {
     if (p->op != ICON_OPERATOR_TOEPLITZ || !p->kt_stale) return ICON_OK;
     const int groups_needed = p->wgroups > 0 ? p->Gcap : 1;
-    if (!p->Kt) ICON_TRY(p->arena.alloc(&p->Kt, (size_t)p->Gcap * p->n0 * p->n1));
+    if (p->Kt && p->kt_cap < groups_needed) {   // one kernel per group needs a larger table
+        p->arena.release(p->Kt);
+        p->Kt = nullptr;
+    }
+    if (!p->Kt) {
+        ICON_TRY(p->arena.alloc(&p->Kt, (size_t)groups_needed * p->n0 * p->n1));
+        p->kt_cap = groups_needed;
+    }
     float *xy_d = nullptr;
     if (!p->nodes_xy) ICON_TRY(p->arena.upload(&p->nodes_xy, p->xy.data(), p->xy.size()));
     xy_d = p->nodes_xy;
@@ -580,17 +606,20 @@ icon_status flush_update(icon_plan *p, cudaStream_t st)
 // y-pass, the fused inverse x-pass / r-hat / forward x-pass of r-hat, the
 // quadratic form's y-pass and the step length.  This iteration's update is
 // left pending (flush_update or the next iteration applies it).
-icon_status launch_iteration_xt(icon_plan *p, int G, bool clamp, int data_type, float thr, double *hist_a,
-                                double *hist_r, cudaStream_t st)
+// The kernels of one such iteration with the deferred update given
+// explicitly: upd applies the previous iteration's update (clamped when
+// clamp_prev) in the forward x-pass.  Changes no host-side state, so it can
+// be captured into a CUDA graph and replayed.
+icon_status launch_iteration_xt_raw(icon_plan *p, int G, bool upd, bool clamp_prev, int data_type, float thr,
+                                    double *hist_a, double *hist_r, cudaStream_t st)
 {
-    if (p->upd_pending && p->upd_G != G) ICON_TRY(flush_update(p, st));
     Geo g = p->geo_unit();
     const double slots = (double)G * p->B;
     const double NN = (double)p->N0 * p->N1, G1b = (double)p->n0 * p->N1 * 8, Kb = (double)p->n0 * p->n1 * 4;
     icon::XtArgs xa{};
     xa.N0 = p->N0; xa.N1 = p->N1; xa.n0 = p->n0; xa.tw0 = p->tw0; xa.G1 = p->G1; xa.m = p->m;
-    xa.rhat_in = p->rhat; xa.alpha = p->alpha; xa.upd = p->upd_pending ? 1 : 0; xa.clamp = p->upd_clamp ? 1 : 0;
-    xa.data_type = p->upd_dtype; xa.thr = p->upd_thr; xa.rhat = p->rhat; xa.Ahwb = p->Ahwb; xa.part_rtr = p->part_rtr;
+    xa.rhat_in = p->rhat; xa.alpha = p->alpha; xa.upd = upd ? 1 : 0; xa.clamp = clamp_prev ? 1 : 0;
+    xa.data_type = data_type; xa.thr = thr; xa.rhat = p->rhat; xa.Ahwb = p->Ahwb; xa.part_rtr = p->part_rtr;
     const double xf_bytes = (xa.upd ? NN * 16 : NN * 4) + G1b;
     dim3 gy(G, p->n0);
     WITH_B(p->B,
@@ -601,6 +630,14 @@ icon_status launch_iteration_xt(icon_plan *p, int G, bool clamp, int data_type, 
                  L::ypass_toep_quad(p->ey, gy, p->thr_y, p->smem_yt, st, g, p->G1, p->part_rtar)))
     LAUNCH(p, K_ALPHA, st, icon::k_alpha<<<G, 32 * p->B, 0, st>>>(p->part_rtr, p->N1, p->part_rtar, p->n0, p->B, p->alpha, hist_a, hist_r));
     ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+icon_status launch_iteration_xt(icon_plan *p, int G, bool clamp, int data_type, float thr, double *hist_a,
+                                double *hist_r, cudaStream_t st)
+{
+    if (p->upd_pending && p->upd_G != G) ICON_TRY(flush_update(p, st));
+    ICON_TRY(launch_iteration_xt_raw(p, G, p->upd_pending, p->upd_clamp, p->upd_dtype, p->upd_thr, hist_a, hist_r, st));
     p->upd_pending = true;
     p->upd_clamp = clamp;
     p->upd_dtype = data_type;
@@ -662,7 +699,8 @@ icon_status run_schedule_tol(icon_plan *p, const icon_solve_cfg *cfg, int G, int
     p->upd_pending = false;
     auto run = [&](int n, bool clamp, bool checked) {
         for (int k = 0; k < n && rc == ICON_OK; ++k) {
-            const bool check = checked && ((k + 1) % check_every == 0 || k + 1 == n);
+            // tol = 0 never stops: only the phase's last step is measured, for h_step
+            const bool check = checked && ((tol > 0.0 && (k + 1) % check_every == 0) || k + 1 == n);
             rc = launch_iteration(p, G, clamp, cfg->data_type, cfg->threshold, nullptr, nullptr, st, check);
             ++done;
             if (rc != ICON_OK || !check) continue;
@@ -680,9 +718,9 @@ icon_status run_schedule_tol(icon_plan *p, const icon_solve_cfg *cfg, int G, int
             if (all) break;
         }
     };
-    run(a, false, false);   // INFR (Iteration2.cu:129-132)
-    run(b, true, true);     // ICON, stopped once every slice's step is within tol
-    run(c, false, false);   // INFR
+    run(a, false, false);      // INFR (Iteration2.cu:129-132)
+    run(b, true, tol > 0.0 || h_step != nullptr);   // ICON, stopped once every slice's step is within tol
+    run(c, false, false);      // INFR
     if (rc == ICON_OK) rc = flush_update(p, st);
     p->upd_pending = false;
     if (done_out) *done_out = done;
@@ -761,7 +799,13 @@ icon_status icon_devices(int *h_count, int *h_sm, int max)
     return ICON_OK;
 }
 
-icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
+static icon_status plan_create_impl(const icon_geometry *geo, int group, icon_plan **out);
+
+icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out) { return plan_create_impl(geo, 0, out); }
+
+// group > 0: slices per group (1, 2, 4 or 8, at most the size's default);
+// 0: the default choice.
+static icon_status plan_create_impl(const icon_geometry *geo, int group, icon_plan **out)
 {
     if (!geo || !out) return fail(ICON_ERR_INVALID, "null argument");
     *out = nullptr;
@@ -794,6 +838,10 @@ icon_status icon_plan_create(const icon_geometry *geo, icon_plan **out)
     if (const char *ov = std::getenv("ICON_BATCH")) {
         int v = atoi(ov);
         if ((v == 1 || v == 2 || v == 4 || v == 8) && v < B) B = v;
+    }
+    if (group > 0) {
+        if (group != 1 && group != 2 && group != 4 && group != 8) return fail(ICON_ERR_INVALID, "group must be 1, 2, 4 or 8");
+        B = std::min(B, group);
     }
     while (B > 1 && B / 2 >= geo->capacity) B /= 2;
     p->B = B;
@@ -1284,7 +1332,7 @@ icon_status icon_solve_until(icon_plan *p, const icon_solve_cfg *cfg, const void
     DeviceGuard guard(p->dev);
     cudaStream_t st = (cudaStream_t)stream;
     const int G = groups(p, S);
-    const size_t tot = (size_t)G * p->N1 * p->N0 * p->B, slots = (size_t)G * p->B;
+    const size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
     ICON_TRY(ensure_toeplitz(p, st));
     LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float2><<<grid1d(tot), 256, 0, st>>>((const float2 *)d_Ahwb, p->Ahwb, S, p->N0, p->N1, p->B, tot));
     if (warm_start) LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float><<<grid1d(tot), 256, 0, st>>>(d_m, p->m, S, p->N0, p->N1, p->B, tot));
@@ -1404,6 +1452,72 @@ icon_status icon_trace_read(icon_plan *p, int *h_count, double *h_ms, double *h_
 }
 
 long long icon_launch_count(const icon_plan *p) { return p ? p->launches : 0; }
+
+}  // extern "C"
+
+// ------------------------------------------------ hooks of icon_batch.cu ----
+namespace iconx {
+
+icon_status plan_create_group(const icon_geometry *geo, int group, icon_plan **out)
+{
+    return plan_create_impl(geo, group, out);
+}
+int plan_group(const icon_plan *p) { return p->B; }
+int plan_capacity(const icon_plan *p) { return p->cap; }
+int plan_device(const icon_plan *p) { return p->dev; }
+float *plan_rows_buffer(icon_plan *p) { return p->rows; }
+float *plan_out_buffer(icon_plan *p) { return p->mout; }
+
+static bool clamp_at(const icon_solve_cfg *cfg, int it)
+{
+    const int a = cfg->infr_before, iters = a + cfg->icon + cfg->infr_after;
+    return a <= it && it < iters - cfg->infr_after;                // Iteration2.cu:129
+}
+
+icon_status plan_stage_in(icon_plan *p, const float *d_rows, int S, cudaStream_t st)
+{
+    ICON_TRY(check_plan(p, S));
+    DeviceGuard guard(p->dev);
+    const int G = groups(p, S);
+    ICON_TRY(launch_rows(p, d_rows, S, G, nullptr, st));
+    ICON_TRY(ensure_toeplitz(p, st));
+    ICON_TRY(launch_adjoint(p, p->f, G, 0, p->Ahwb, st));
+    ICON_CUDA(cudaMemsetAsync(p->m, 0, (size_t)G * p->N1 * p->N0 * p->B * sizeof(float), st));
+    p->upd_pending = false;
+    return ICON_OK;
+}
+
+icon_status plan_iteration(icon_plan *p, int S, int it, const icon_solve_cfg *cfg, cudaStream_t st)
+{
+    const int G = groups(p, S);
+    if (p->op == ICON_OPERATOR_TOEPLITZ && p->xt_ok)
+        return launch_iteration_xt_raw(p, G, it > 0, it > 0 && clamp_at(cfg, it - 1), cfg->data_type, cfg->threshold,
+                                       nullptr, nullptr, st);
+    return launch_iteration(p, G, clamp_at(cfg, it), cfg->data_type, cfg->threshold, nullptr, nullptr, st);
+}
+
+icon_status plan_stage_out(icon_plan *p, int S, const icon_solve_cfg *cfg, float *d_out, cudaStream_t st)
+{
+    DeviceGuard guard(p->dev);
+    const int iters = cfg->infr_before + cfg->icon + cfg->infr_after;
+    if (p->op == ICON_OPERATOR_TOEPLITZ && p->xt_ok && iters > 0) {
+        p->upd_pending = true;
+        p->upd_clamp = clamp_at(cfg, iters - 1);
+        p->upd_dtype = cfg->data_type;
+        p->upd_thr = cfg->threshold;
+        p->upd_G = groups(p, S);
+        ICON_TRY(flush_update(p, st));
+    }
+    LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float><<<grid1d((size_t)S * p->N0 * p->N1), 256, 0, st>>>(p->m, d_out, S, p->N0, p->N1, p->B));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
+}
+
+icon_status fail_msg(icon_status st, const std::string &msg) { return fail(st, msg); }
+
+}  // namespace iconx
+
+extern "C" {
 
 // Lets the other translation units of the library report through
 // icon_last_error().

@@ -81,7 +81,8 @@ static void xt_go(int mode, cudaStream_t st, int G, const XtArgs &a)
     const dim3 grid((unsigned)(a.N1 * (B / BH)), (unsigned)G);
     const size_t smem = xtoep_smem(S::N, BH);
     if (mode == 0) k_xtoep<B, BH, LA, LNB, 0><<<grid, S::T, smem, st>>>(a);
-    else k_xtoep<B, BH, LA, LNB, 1><<<grid, S::T, smem, st>>>(a);
+    else if (mode == 1) k_xtoep<B, BH, LA, LNB, 1><<<grid, S::T, smem, st>>>(a);
+    else k_xtoep<B, BH, LA, LNB, 2><<<grid, S::T, smem, st>>>(a);
 }
 template <int B, int BH, int LA, int LNB>
 static cudaError_t xt_attr()
@@ -89,6 +90,9 @@ static cudaError_t xt_attr()
     const int bytes = (int)xtoep_smem(XtShape<BH, LA, LNB>::N, BH);
     cudaError_t e = cudaFuncSetAttribute((const void *)k_xtoep<B, BH, LA, LNB, 0>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute((const void *)k_xtoep<B, BH, LA, LNB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bytes);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute((const void *)k_xtoep<B, BH, LA, LNB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 bytes);
@@ -206,58 +210,61 @@ void Launch<B>::update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat,
     else k_update<B, false><<<grid, 256, 0, st>>>(m, rhat, alpha, per_group, clamp, data_type, thr);
 }
 
+// The dynamic shared-memory limit is a property of the kernel function, not
+// of a plan: plans of different sizes share the variants of one B, so every
+// variant gets the device's opt-in maximum (what a launch actually asks for
+// still sets the occupancy).  Lowering it to one plan's size would make a
+// larger plan's next launch fail.
 template <int B>
-cudaError_t Launch<B>::set_smem(int ex, int ey, size_t smem_x, size_t need_x, size_t smem_y, size_t smem_ya,
-                                size_t smem_yt)
+cudaError_t Launch<B>::set_smem(int ex, int ey, size_t, size_t, size_t, size_t, size_t)
 {
-    cudaError_t e = cudaSuccess;
-    auto set = [&](const void *fn, size_t bytes) {
-        cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    auto set = [&](const void *fn) {
+        cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
         if (r != cudaSuccess && e == cudaSuccess) e = r;
     };
-    if (ex == 32) {
-        set((const void *)k_xpass_fwd<true, B, 32>, smem_x);
-        set((const void *)k_xpass_fwd<false, B, 32>, smem_x);
-        set((const void *)k_xpass_fwd_r2c<B, 32>, smem_x / 2);
-        set((const void *)k_xpass_fwd_r2c<B, 32, true>, smem_x / 2);
-        set((const void *)k_xpass_fwd<true, B, 32, true>, smem_x);
-        set((const void *)k_xpass_adj<0, B, 32>, need_x);
-        set((const void *)k_xpass_adj<1, B, 32>, need_x);
-        set((const void *)k_rows_fwd<B, 32>, smem_x);
-        set((const void *)k_row_adj<B, 32>, smem_x);
-    } else {
-        set((const void *)k_xpass_fwd<true, B, 16>, smem_x);
-        set((const void *)k_xpass_fwd<false, B, 16>, smem_x);
-        set((const void *)k_xpass_fwd_r2c<B, 16>, smem_x / 2);
-        set((const void *)k_xpass_fwd_r2c<B, 16, true>, smem_x / 2);
-        set((const void *)k_xpass_fwd<true, B, 16, true>, smem_x);
-        set((const void *)k_xpass_adj<0, B, 16>, need_x);
-        set((const void *)k_xpass_adj<1, B, 16>, need_x);
-        set((const void *)k_rows_fwd<B, 16>, smem_x);
-        set((const void *)k_row_adj<B, 16>, smem_x);
-    }
-    set((const void *)k_ytoep4<B, 2, 0>, ytoep4_smem(128, B));
-    set((const void *)k_ytoep4<B, 3, 0>, ytoep4_smem(256, B));
-    set((const void *)k_ytoep4<B, 4, 0>, ytoep4_smem(512, B));
-    set((const void *)k_ytoep4<B, 5, 0>, ytoep4_smem(1024, B));
-    set((const void *)k_ytoep4<B, 2, 1>, ytoep4_smem(128, B));
-    set((const void *)k_ytoep4<B, 3, 1>, ytoep4_smem(256, B));
-    set((const void *)k_ytoep4<B, 4, 1>, ytoep4_smem(512, B));
-    set((const void *)k_ytoep4<B, 5, 1>, ytoep4_smem(1024, B));
-    if (ey == 32) {
-        set((const void *)k_ypass_fwd<B, 32, false>, smem_y);
-        set((const void *)k_ypass_fwd<B, 32, true>, smem_y);
-        set((const void *)k_ypass_adj<B, 32, false>, smem_ya);
-        set((const void *)k_ypass_toep<B, 32>, smem_yt);
-        set((const void *)k_ypass_toep_quad<B, 32>, smem_yt);
-    } else {
-        set((const void *)k_ypass_fwd<B, 16, false>, smem_y);
-        set((const void *)k_ypass_fwd<B, 16, true>, smem_y);
-        set((const void *)k_ypass_adj<B, 16, false>, smem_ya);
-        set((const void *)k_ypass_adj<B, 16, true>, smem_ya);
-        set((const void *)k_ypass_toep<B, 16>, smem_yt);
-        set((const void *)k_ypass_toep_quad<B, 16>, smem_yt);
-    }
+    (void)ex;
+    (void)ey;
+    set((const void *)k_xpass_fwd<true, B, 32>);
+    set((const void *)k_xpass_fwd<false, B, 32>);
+    set((const void *)k_xpass_fwd_r2c<B, 32>);
+    set((const void *)k_xpass_fwd_r2c<B, 32, true>);
+    set((const void *)k_xpass_fwd<true, B, 32, true>);
+    set((const void *)k_xpass_adj<0, B, 32>);
+    set((const void *)k_xpass_adj<1, B, 32>);
+    set((const void *)k_rows_fwd<B, 32>);
+    set((const void *)k_row_adj<B, 32>);
+    set((const void *)k_xpass_fwd<true, B, 16>);
+    set((const void *)k_xpass_fwd<false, B, 16>);
+    set((const void *)k_xpass_fwd_r2c<B, 16>);
+    set((const void *)k_xpass_fwd_r2c<B, 16, true>);
+    set((const void *)k_xpass_fwd<true, B, 16, true>);
+    set((const void *)k_xpass_adj<0, B, 16>);
+    set((const void *)k_xpass_adj<1, B, 16>);
+    set((const void *)k_rows_fwd<B, 16>);
+    set((const void *)k_row_adj<B, 16>);
+    set((const void *)k_ypass_fwd<B, 32, false>);
+    set((const void *)k_ypass_fwd<B, 32, true>);
+    set((const void *)k_ypass_adj<B, 32, false>);
+    set((const void *)k_ypass_toep<B, 32>);
+    set((const void *)k_ypass_toep_quad<B, 32>);
+    set((const void *)k_ypass_fwd<B, 16, false>);
+    set((const void *)k_ypass_fwd<B, 16, true>);
+    set((const void *)k_ypass_adj<B, 16, false>);
+    set((const void *)k_ypass_adj<B, 16, true>);
+    set((const void *)k_ypass_toep<B, 16>);
+    set((const void *)k_ypass_toep_quad<B, 16>);
+    set((const void *)k_ytoep4<B, 2, 0>);
+    set((const void *)k_ytoep4<B, 3, 0>);
+    set((const void *)k_ytoep4<B, 4, 0>);
+    set((const void *)k_ytoep4<B, 5, 0>);
+    set((const void *)k_ytoep4<B, 2, 1>);
+    set((const void *)k_ytoep4<B, 3, 1>);
+    set((const void *)k_ytoep4<B, 4, 1>);
+    set((const void *)k_ytoep4<B, 5, 1>);
     return e;
 }
 

@@ -1446,9 +1446,11 @@ struct XtArgs {
     const double *alpha;     // update: [G*B] step lengths
     int upd, clamp, data_type;
     float thr;
-    float2 *rhat;            // mid: r-hat out, [G][N1][N0][B]
-    const float2 *Ahwb;      // mid: [G][N1][N0][B]
-    double *part_rtr;        // mid: [G][N1][B] partial |r-hat|^2 per column
+    float2 *rhat;            // mid / adjoint: r-hat (or the adjoint) out, [G][N1][N0][B]
+    const float2 *Ahwb;      // mid / adjoint with resid: [G][N1][N0][B]
+    double *part_rtr;        // mid / adjoint with resid: [G][N1][B] partial |r-hat|^2 per column
+    const float *rcx, *rcy;  // adjoint: deapodisation reciprocals 1/cx [N0], 1/cy [N1]
+    int resid;               // adjoint: subtract Ahwb and sum |.|^2 (else the plain adjoint)
 };
 
 template <int BH, int LA, int LNB>
@@ -1612,7 +1614,10 @@ __device__ __forceinline__ void xt_inverse(float2 (&v)[32 >> LA][1 << LA], float
 // MODE 0: G1 <- F_x(pad m) for every row, m first updated (upd: m <- m -
 // alpha Re r-hat_in, clamped on ICON steps, as k_update).  MODE 1: r-hat =
 // crop F_x^-1(G1) - Ahwb (stored, |r-hat|^2 partial sums per column), then
-// G1 <- F_x(pad r-hat) in place.  Grid: (N1 * B/BH, G), half-group fastest.
+// G1 <- F_x(pad r-hat) in place.  MODE 2: the last x-pass of the NUFFT
+// adjoint (k_xpass_adj's work): out = crop F_x^-1(G1) / (cx cy), with resid
+// minus Ahwb and the |.|^2 partial sums.  Grid: (N1 * B/BH, G), half-group
+// fastest.
 template <int B, int BH, int LA, int LNB, int MODE>
 __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>::T >= 256) ? 2 : 4)
     k_xtoep(XtArgs g)
@@ -1629,7 +1634,7 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
     const size_t ibase = ((size_t)grp * N1 + Y) * N0 * B + bsl;        // image point X at ibase + X*B
     float2 v[S::NI1][NA];
     float2 *As = s + S::N * BH + S::T;   // mid: this CTA's Ahwb column, [N0][BH]
-    if constexpr (MODE == 1) {
+    if constexpr (MODE >= 1) {
         // The G1 column (n0 rows of BH values, rows N1*B float2 apart) into s
         // as [x][BH], then the Ahwb column, staged while the inverse runs.
         const float2 *gsrc = g.G1 + ((size_t)grp * n * N1 + Y) * B + h * BH;
@@ -1643,15 +1648,17 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
             for (int x = t; x < n; x += S::T) cp_async<8>(s + x, gsrc + (size_t)x * rstride);
         }
         cp_async_commit();
-        const float2 *src = g.Ahwb + ((size_t)grp * N1 + Y) * N0 * B + h * BH;
-        if constexpr (BH >= 2) {
-            constexpr int P = BH / 2;                     // 16-byte pieces per point
-            for (int idx = t; idx < N0 * P; idx += S::T) {
-                const int X = idx / P, c = idx - X * P;
-                cp_async<16>(As + X * BH + 2 * c, src + (size_t)X * B + 2 * c);
+        if (MODE == 1 || g.resid) {
+            const float2 *src = g.Ahwb + ((size_t)grp * N1 + Y) * N0 * B + h * BH;
+            if constexpr (BH >= 2) {
+                constexpr int P = BH / 2;                     // 16-byte pieces per point
+                for (int idx = t; idx < N0 * P; idx += S::T) {
+                    const int X = idx / P, c = idx - X * P;
+                    cp_async<16>(As + X * BH + 2 * c, src + (size_t)X * B + 2 * c);
+                }
+            } else {
+                for (int X = t; X < N0; X += S::T) cp_async<8>(As + X, src + (size_t)X * B);
             }
-        } else {
-            for (int X = t; X < N0; X += S::T) cp_async<8>(As + X, src + (size_t)X * B);
         }
         cp_async_commit();
     }
@@ -1714,6 +1721,42 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
         }
         __syncthreads();   // the staged m is read before step 1 rewrites s
         xt_forward<BH, LA, LNB>(v, s, u, sl, g.tw0, col, rstride);
+    } else if constexpr (MODE == 2) {
+        cp_async_wait<1>();
+        __syncthreads();
+        xt_inverse<BH, LA, LNB>(v, s, u, sl, g.tw0);
+        cp_async_wait<0>();
+        __syncthreads();
+        const float rcyY = g.rcy[Y];
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < S::NI1; ++i) {
+            const int tau = u + U * i;
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+                const int X = (32 * NB * a + tau + half) & (n - 1);
+                if (X < N0) {
+                    const float r = g.rcx[X] * rcyY;         // as k_xpass_adj
+                    float2 o = make_float2(v[i][a].x * r, v[i][a].y * r);
+                    if (g.resid) {
+                        const float2 av = As[X * BH + sl];
+                        o.x = o.x - av.x;
+                        o.y = o.y - av.y;
+                        acc += (double)o.x * (double)o.x + (double)o.y * (double)o.y;
+                    }
+                    g.rhat[ibase + (size_t)X * B] = o;
+                }
+            }
+        }
+        if (g.resid) {
+            red[t] = acc;
+            __syncthreads();
+            for (int stride = S::T >> 1; stride >= BH; stride >>= 1) {
+                if (t < stride) red[t] += red[t + stride];
+                __syncthreads();
+            }
+            if (t < BH) g.part_rtr[((size_t)grp * N1 + Y) * B + h * BH + t] = red[t];
+        }
     } else {
         cp_async_wait<1>();    // the column group (Ahwb may still be landing)
         __syncthreads();

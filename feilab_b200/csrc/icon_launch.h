@@ -38,10 +38,11 @@ struct Launch {
                         const float2 *f, float *out, int S);
     static void update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat, const double *alpha, int per_group,
                        int clamp, int data_type, float thr, double *step_part = nullptr);
-    // Toeplitz x-passes (k_xtoep) over G groups: mode 0 the forward of the
-    // real image (with the fused update when a.upd), mode 1 the inverse, r-hat
-    // and the forward of r-hat.  Returns false when n0 has no variant (the
-    // caller then uses the Stockham x-passes).
+    // Three-step x-passes (k_xtoep) over G groups: mode 0 the Toeplitz forward
+    // of the real image (with the fused update when a.upd), mode 1 the
+    // Toeplitz inverse, r-hat and forward of r-hat, mode 2 the NUFFT adjoint's
+    // x-pass (deapodised, optionally minus Ahwb with |.|^2 sums).  Returns
+    // false when n0 has no variant (the caller then uses the Stockham kernels).
     static bool xtoep(int mode, cudaStream_t st, int G, const XtArgs &a);
     // Raises the shared-memory limit of the k_xtoep variants for n0.
     static cudaError_t xtoep_prepare(int n0);

@@ -272,14 +272,20 @@ icon_status icon_mask_create(int n, const float *tilts, int ntilt, float rate05,
     if (cudaMemcpy(m->tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(m->M, full.data(), sizeof(float) * full.size(), cudaMemcpyHostToDevice) != cudaSuccess)
         return mask_fail(ICON_ERR_CUDA, "icon_mask_create: copy of the filter");
-    const size_t smem = sizeof(float2) * 2 * n;
-    cudaError_t e = cudaSuccess;
-    if (m->E == 32) {
-        e = cudaFuncSetAttribute(k_mask_cols<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mask_rows_fwd<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mask_rows_inv<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    } else {
-        e = cudaFuncSetAttribute(k_mask_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // The limit belongs to the kernel function, shared by masks of every
+    // size: raise it to the device's opt-in maximum rather than to this
+    // mask's need, which would lower it under a larger mask made earlier.
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess && (size_t)optin < sizeof(float2) * 2 * n)
+        return mask_fail(ICON_ERR_INVALID, "icon_mask_create: slice too large for shared memory");
+    if (e == cudaSuccess && m->E == 32) {
+        e = cudaFuncSetAttribute(k_mask_cols<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mask_rows_fwd<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mask_rows_inv<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    } else if (e == cudaSuccess) {
+        e = cudaFuncSetAttribute(k_mask_cols<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     }
     if (e != cudaSuccess) return mask_fail(ICON_ERR_CUDA, std::string("icon_mask_create: ") + cudaGetErrorString(e));
     *out = m.release();

@@ -58,6 +58,11 @@ def lib():
         L.icon_plan_set_group_weights.argtypes = [P, V, I]
         L.icon_plan_set_operator.argtypes = [P, I]
         L.icon_plan_set_stop.argtypes = [P, ctypes.c_double, I]
+        L.icon_reproject_host.argtypes = [P, V, F, V, I, V]
+        L.icon_batch_create.argtypes = [V, I, I, I, ctypes.c_char_p, I, ctypes.POINTER(V)]
+        L.icon_batch_destroy.argtypes = [V]
+        L.icon_batch_tuning.argtypes = [V, I, V]
+        L.icon_batch_reconstruct_host.argtypes = [V, ctypes.POINTER(SolveCfg), V, V, I]
         L.icon_trace_enable.argtypes = [P, I]
         L.icon_trace_read.argtypes = [P, V, V, V]
         L.icon_launch_count.argtypes = [P]
@@ -69,7 +74,8 @@ def lib():
                      "icon_reconstruct_host", "icon_trace_enable", "icon_trace_read", "icon_prepare_rhs_stack",
                      "icon_reconstruct_stack", "icon_reconstruct_stack_host", "icon_host_alloc", "icon_host_free",
                      "icon_stack_upload", "icon_device_free", "icon_weights", "icon_plan_set_group_weights",
-                     "icon_plan_set_operator", "icon_plan_set_stop"):
+                     "icon_plan_set_operator", "icon_plan_set_stop", "icon_reproject_host", "icon_batch_create",
+                     "icon_batch_destroy", "icon_batch_tuning", "icon_batch_reconstruct_host"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -405,3 +411,69 @@ def weights(nx, tilts):
     w = np.zeros((len(t), int(nx)), np.float32)
     _check(lib().icon_weights(int(nx), len(t), t.ctypes.data_as(ctypes.c_void_p), w.ctypes.data_as(ctypes.c_void_p)))
     return w
+
+
+class Series(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("thickness", ctypes.c_int), ("ntilt", ctypes.c_int),
+                ("tilt_deg", ctypes.POINTER(ctypes.c_float)), ("slices", ctypes.c_int)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("group", ctypes.c_int), ("chunk", ctypes.c_int), ("us_per_slice_iteration", ctypes.c_double),
+                ("tuned", ctypes.c_int)]
+
+
+class IconBatch:
+    """Many tilt series of uneven shape reconstructed together
+    (include/icon_batch.h): `series` is a list of (nx, thickness, tilts,
+    slices).  tune: 0 = cache file or defaults, 1 = time shapes missing from
+    the cache, 2 = also append them to the cache file."""
+
+    def __init__(self, series, device=None, operator="toeplitz", tune_cache=None, tune=0):
+        import torch
+        if device is None:
+            device = torch.cuda.current_device()
+        self.device = torch.device("cuda", device)
+        self._tilts = [np.ascontiguousarray(np.asarray(t, np.float32)) for _, _, t, _ in series]
+        arr = (Series * len(series))()
+        for k, (nx, th, _, sl) in enumerate(series):
+            t = self._tilts[k]
+            arr[k] = Series(int(nx), int(th), len(t), t.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(sl))
+        self.shapes = [(int(nx), int(th) or int(nx), len(self._tilts[k]), int(sl))
+                       for k, (nx, th, _, sl) in enumerate(series)]
+        h = ctypes.c_void_p()
+        self._destroy = lib().icon_batch_destroy
+        _check(lib().icon_batch_create(arr, len(series), int(device), IconPlan.OPERATORS[operator],
+                                       tune_cache.encode() if tune_cache else None, int(tune), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._destroy(h)
+            self._h = None
+
+    __del__ = close
+
+    def tuning(self, k):
+        t = Tuning()
+        _check(lib().icon_batch_tuning(self._h, int(k), ctypes.byref(t)))
+        return {"group": t.group, "chunk": t.chunk, "us_per_slice_iteration": t.us_per_slice_iteration,
+                "tuned": t.tuned}
+
+    def reconstruct(self, rows, iters=(0, 10, 0), data_type=1, threshold=0.03, out=None, concurrent=True):
+        """rows: per series a host float32 array or tensor (slices, ntilt, nx),
+        best pinned; returns per series (slices, N0, N1) float32 host tensors
+        (pinned), or fills `out`."""
+        import torch
+        rows = [torch.as_tensor(np.ascontiguousarray(r, np.float32)) if not torch.is_tensor(r) else r.contiguous()
+                for r in rows]
+        if out is None:
+            out = [torch.empty((sl, nx, th), dtype=torch.float32, pin_memory=True) for nx, th, _, sl in self.shapes]
+        n = len(self.shapes)
+        rp = (ctypes.c_void_p * n)(*[r.data_ptr() for r in rows])
+        op = (ctypes.c_void_p * n)(*[o.data_ptr() for o in out])
+        a, b, c = iters
+        cfg = SolveCfg(int(a), int(b), int(c), int(data_type), float(threshold))
+        _check(lib().icon_batch_reconstruct_host(self._h, ctypes.byref(cfg), rp, op, int(bool(concurrent))))
+        return out

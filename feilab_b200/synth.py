@@ -178,3 +178,35 @@ def series(config: str, device="cpu", ys=None, seed=None):
     rows = project(ph, tilts, ys=ys, device=device)
     rows = add_noise(rows, snr, sd)
     return rows, tilts, shape[2], dict(shape=shape, ellipsoids=E, blobs=G, background=bg, snr=snr, seed=sd)
+
+
+def uneven_batch(n_series=24, seed=3003, slice_scale=1.0, device="cpu"):
+    """The uneven multi-series workload: n_series seeded tilt series with
+    width drawn from {256, 512, 768, 1024, 2048}, slice count uniform in
+    [64, 512] (times slice_scale, at least 1), thickness uniform in
+    [100, 400], tilt range +-U[45, 70] deg with step U[1.5, 3] deg and 10% of
+    the tilts dropped at random, phantoms of ellipsoids and Gaussian blobs
+    (counts scaled from the 1024x1024x300 production phantom's 300 and 3000 by
+    volume, at least 20 and 100) on a 0.1 background, Gaussian noise at SNR
+    U[0.1, 0.5].  Returns a list of dicts with nx, thickness, tilts, slices,
+    rows (slices, ntilt, nx) float32 and snr."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_series):
+        nx = int(rng.choice([256, 512, 768, 1024, 2048]))
+        slices = max(1, int(round(int(rng.integers(64, 513)) * slice_scale)))
+        thick = int(rng.integers(100, 401))
+        rng_deg = float(rng.uniform(45.0, 70.0))
+        step = float(rng.uniform(1.5, 3.0))
+        n = int(math.floor(2 * rng_deg / step)) + 1
+        tilts = (-rng_deg + step * np.arange(n)).astype(np.float32)
+        keep = np.sort(rng.choice(n, size=n - int(round(0.1 * n)), replace=False))
+        tilts = tilts[keep]
+        snr = float(rng.uniform(0.1, 0.5))
+        vol = nx * slices * thick / (1024.0 * 1024.0 * 300.0)
+        E, G = max(20, int(round(300 * vol))), max(100, int(round(3000 * vol)))
+        sd = int(seed) * 1000 + k
+        ph = make_phantom((nx, slices, thick), E, G, seed=sd, background=0.1)
+        rows = add_noise(project(ph, tilts, device=device), snr, sd)
+        out.append(dict(nx=nx, thickness=thick, tilts=tilts, slices=slices, rows=rows, snr=snr))
+    return out
