@@ -37,6 +37,10 @@ to step, so 20 steps run one whole reconstruction of the sample.  value =
 slices x (steps / 20) / measured time.  The repo arm's cpu_baseline runs the
 same sample through all 20 pieces, timed as a whole.
 
+window_kb4: the same workload with the Kaiser-Bessel window of half-width 4
+(8 taps per dimension instead of the reference's 14-tap Gaussian): both
+operators' slices/s, its NUFFT pair and its parity record.
+
 Also in the repo arm's line: reference_gpu (the reference's own ICON-GPU,
 compiled from its sources for sm_100a into oracle/_ref/, run by wall clock
 on a 64-slice stack of the workload, and the agreement of its slices with
@@ -363,7 +367,7 @@ def run_ours(args):
     except Exception:
         pass
 
-    def timed_device(op, steps):
+    def timed_device(op, steps, plan=plan):
         """Device-resident rows in, `steps` timed steps (input stage +
         schedule), CUDA events on the launch stream, max over ranks."""
         plan.set_operator(op)
@@ -435,12 +439,28 @@ def run_ours(args):
     # NUFFT pair (forward R2C + adjoint) per slice-iteration: the model bytes
     # of the reference's staged NUFFT over the time of our fused kernels, from
     # the run with the NUFFT operator.
-    tn = runs["nufft"]["trace"]
-    fwd_ms = (tn["xpass_fwd"][1] + tn["ypass_fwd"][1] + tn["interp_fin"][1]) / 2.0
-    adj_ms = tn["ypass_adj"][1] + tn["xpass_adj"][1]
-    slice_iters = slots * runs["nufft"]["steps"] * sum(SCHED)
-    pair_s = (fwd_ms + adj_ms) / 1e3 / slice_iters
-    pair_gbs = PAIR_MODEL_BYTES / pair_s / 1e9
+    def pair(run):
+        tn = run["trace"]
+        fwd_ms = (tn["xpass_fwd"][1] + tn["ypass_fwd"][1] + tn["interp_fin"][1]) / 2.0
+        adj_ms = tn["ypass_adj"][1] + tn["xpass_adj"][1]
+        slice_iters = slots * run["steps"] * sum(SCHED)
+        pair_s = (fwd_ms + adj_ms) / 1e3 / slice_iters
+        pair_gbs = PAIR_MODEL_BYTES / pair_s / 1e9
+        return {"model_bytes_per_slice": PAIR_MODEL_BYTES, "gbs": round(pair_gbs, 1),
+                "frac": round(pair_gbs / peak, 4), "us_per_slice": round(pair_s * 1e6, 3)}
+    # FP32 work of the dominant Toeplitz y-pass (its bound is the FP32 pipe, not
+    # DRAM): per slot two complex FFTs of n1 points (5 n log2 n flops each) per
+    # grid row, against the SIMT FP32 peak of the device at the sampled clock.
+    fp32 = None
+    if dom == "ypass_toep":
+        import math
+        props = torch.cuda.get_device_properties(local)
+        mhz = (head["clocks"] or {}).get("sm_max_mhz") or 1965.0
+        peak_tf = props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
+        flops = slots * n0 * 2 * 5 * n1 * math.log2(n1)
+        tf = flops / (ms / cnt / 1e3) / 1e12
+        fp32 = {"model_flops_per_launch": flops, "achieved_tflops": round(tf, 2), "peak_tflops": round(peak_tf, 1),
+                "frac": round(tf / peak_tf, 4), "peak_source": "SMs x 128 FP32 lanes x 2 x max SM clock"}
 
     line = {"metric": METRIC, "value": value, "unit": "slices/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
@@ -453,9 +473,8 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "traffic": (traffic_slot * slots if traffic_slot else None),
-                         "algorithmic_bytes_per_launch": by / cnt},
-            "nufft_pair": {"model_bytes_per_slice": PAIR_MODEL_BYTES, "gbs": round(pair_gbs, 1),
-                           "frac": round(pair_gbs / peak, 4), "us_per_slice": round(pair_s * 1e6, 3)},
+                         "algorithmic_bytes_per_launch": by / cnt, "fp32": fp32},
+            "nufft_pair": pair(runs["nufft"]),
             "kernels": kernel_table(trace),
             "e2e": {"value": e2e, "unit": "slices/s", "h2d_bytes_per_step": int(S * len(tilts) * NX * 4),
                     "d2h_bytes_per_step": int(S * NX * THICK * 4)},
@@ -465,6 +484,21 @@ def run_ours(args):
                                "ms_per_step": r["t"] / r["steps"] * 1e3,
                                "kernels": kernel_table(r["trace"]), "clocks": r["clocks"]} for op, r in runs.items()}}
     plan.set_operator(args.operator)
+    if not args.no_kb:
+        # The Kaiser-Bessel window mode (half-width 4, 8 taps): both operators
+        # over min(K, 3) steps on the same rows, its NUFFT pair, and its result
+        # on the parity slices against the reference's and the FP64 oracle's
+        # (both Gaussian).
+        kplan = icon.IconPlan(NX, THICK, tilts, capacity=S, device=local, window="kb4")
+        kruns = {op: timed_device(op, min(args.steps, 3), plan=kplan) for op in ("toeplitz", "nufft")}
+        kplan.close()
+        line["window_kb4"] = {op: {"value": r["value"], "steps": r["steps"], "ms_per_step": r["t"] / r["steps"] * 1e3,
+                                   "kernels": kernel_table(r["trace"])} for op, r in kruns.items()}
+        line["window_kb4"]["nufft_pair"] = pair(kruns["nufft"])
+        if rank == 0:
+            line["window_kb4"]["parity"] = {
+                op: parity_leg(lambda n: icon.IconPlan(NX, THICK, tilts, capacity=n, device=local, window="kb4"), op)
+                for op in ops}
     line["warm_start"] = warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S)
     if rank == 0:
         line["parity"] = {op: parity_leg(lambda n: icon.IconPlan(NX, THICK, tilts, capacity=n, device=local), op)
@@ -631,6 +665,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference ICON-GPU leg")
+    ap.add_argument("--no-kb", action="store_true", help="skip the Kaiser-Bessel window leg")
     ap.add_argument("--operator", default="toeplitz", choices=["nufft", "toeplitz"],
                     help="normal operator of the headline run (the other is timed beside it)")
     ap.add_argument("--uneven-scale", type=float, default=0.25,

@@ -25,11 +25,12 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.pa
 LIB_UNITS = [("icon_api.cu", [], "icon_api.o"), ("icon_noalloc.cu", [], "icon_noalloc.o"),
              ("ws_api.cu", [], "ws_api.o"), ("ws_net.cu", [], "ws_net.o"),
              ("tools.cu", [], "tools.o"), ("mask.cu", [], "mask.o"),
-             ("frc.cu", [], "frc.o"), ("loo.cu", [], "loo.o"), ("icon_batch.cu", [], "icon_batch.o")] + [
+             ("frc.cu", [], "frc.o"), ("loo.cu", [], "loo.o"), ("icon_batch.cu", [], "icon_batch.o"),
+             ("icon_warm.cu", [], "icon_warm.o")] + [
     ("icon_kern_b.cu", ["-DICON_KB=%d" % b], "icon_kern_b%d.o" % b) for b in (1, 2, 4, 8)]
 LIB_DEPS = ["icon_api.cu", "icon_noalloc.cu", "icon_kern_b.cu", "icon_launch.h", "icon_kernels.cuh", "icon_device.cuh",
             "ws_api.cu", "ws_conv.cuh", "ws_tc.cuh", "ws_net.cu", "ws_kernels.cuh", "tools.cu", "mask.cu", "frc.cu", "loo.cu",
-            "icon_batch.cu", "icon_internal.h"]
+            "icon_batch.cu", "icon_internal.h", "icon_warm.cu"]
 BUILD_DIR = os.path.join(HERE, "_build")
 # Command-line tools: executable -> sources (host C++ over the C ABI).
 TOOLS = {"icon-gpu": ["icon_cli.cpp", "mrc_io.cpp"], "icon-preprocess": ["preprocess_cli.cpp", "mrc_io.cpp"],

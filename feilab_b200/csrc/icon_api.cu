@@ -95,16 +95,45 @@ void weights(int nx, int nz, const float *t, float *w)
         }
 }
 
-// Deapodisation factors (NU:22-42): exp(-b (pi k/n)^2) in double, stored as float.
-std::vector<float> deapod(int N, int n, float b)
+// Modified Bessel function I0 by its power series sum_k ((x/2)^k / k!)^2
+// (positive terms; converges to double precision well within 60 terms for
+// the arguments of the Kaiser-Bessel window, x <= 4 * 2 pi).
+double bessel_i0(double x)
+{
+    double term = 1.0, sum = 1.0, q = 0.25 * x * x;
+    for (int k = 1; k < 60; ++k) {
+        term *= q / ((double)k * (double)k);
+        sum += term;
+        if (term < 1e-18 * sum) break;
+    }
+    return sum;
+}
+
+// Shape parameter of the Kaiser-Bessel window for oversampling theta:
+// kb = pi (2 - 1/theta) (the choice of Potts, Steidl and Tasche's NFFT).
+double kb_shape(float theta) { return M_PI * (2.0 - 1.0 / (double)theta); }
+
+// Deapodisation factors (NU:22-42): exp(-b (pi k/n)^2) in double, stored as
+// float.  Kaiser-Bessel (kb > 0): the window's Fourier transform
+// I0(K sqrt(kb^2 - (2 pi k/n)^2)) / I0(kb K), real for theta >= 1.
+std::vector<float> deapod(int N, int n, float b, double kb = 0.0)
 {
     std::vector<float> c(N);
+    const double i0m = kb > 0.0 ? bessel_i0(kb * icon::kKbHalf) : 1.0;
     for (int X = 0; X < N; ++X) {
         int k = X - N / 2;
-        c[X] = (float)std::exp(-(double)b * ((kRefPi * k / (double)n) * (kRefPi * k / (double)n)));
+        if (kb > 0.0) {
+            double w = 2.0 * M_PI * k / (double)n;
+            c[X] = (float)(bessel_i0(icon::kKbHalf * std::sqrt(kb * kb - w * w)) / i0m);
+        } else {
+            c[X] = (float)std::exp(-(double)b * ((kRefPi * k / (double)n) * (kRefPi * k / (double)n)));
+        }
     }
     return c;
 }
+
+// 1 / (pi I0(kb K)): the Kaiser-Bessel window's scale (0 for the Gaussian).
+double kb_inv(double kb) { return kb > 0.0 ? 1.0 / (M_PI * bessel_i0(kb * icon::kKbHalf)) : 0.0; }
 
 std::vector<float2> twiddles(int n)
 {
@@ -174,6 +203,7 @@ struct Arena {
 // Node tables of one geometry (a tilt series or a single reprojection line).
 struct NodeTables {
     int M = 0;
+    int taps = 0;    // x taps with entries per node (14, or 8 for Kaiser-Bessel)
     float *phix = nullptr, *phiy = nullptr, *w = nullptr;
     int *ix0 = nullptr, *iy0 = nullptr, *row_off = nullptr, *ent_jt = nullptr, *ent_iy0 = nullptr;
     unsigned short *ent_lb = nullptr;
@@ -185,6 +215,9 @@ struct NodeTables {
 struct icon_plan {
     int dev = 0;
     int nx = 0, N0 = 0, N1 = 0, nz = 0, M = 0, n0 = 0, n1 = 0, lg0 = 0, lg1 = 0;
+    int window = ICON_WINDOW_GAUSS6;
+    int tlo = 0, thi = icon::kTaps - 1;     // taps of the window that can be non-zero
+    double kb0 = 0.0, kb1 = 0.0;            // Kaiser-Bessel shape per dimension (0: Gaussian)
     int B = 1, cap = 0, Gcap = 0;
     float th0 = 0, th1 = 0, b0 = 0, bf0 = 0, b1 = 0, bf1 = 0;
     std::vector<float> tlt, th_neg, xy, w;
@@ -265,6 +298,7 @@ struct icon_plan {
         Geo g;
         g.N0 = N0; g.N1 = N1; g.n0 = n0; g.n1 = n1; g.lg0 = lg0; g.lg1 = lg1;
         g.M = t.M; g.nx = nx; g.nz = nz; g.B = B;
+        g.tlo = tlo; g.thi = thi;
         g.w = t.w; g.wstride = 0;
         if (&t == &nodes && wgroups > 0) {   // icon_plan_set_group_weights
             g.w = wgroup;
@@ -357,24 +391,27 @@ icon_status build_tables(icon_plan *p, const float *xy, const float *w, int M, N
     ICON_TRY(p->arena.alloc(&t.ix0, (size_t)M));
     ICON_TRY(p->arena.alloc(&t.iy0, (size_t)M));
     int blk = 256, grd = (M + blk - 1) / blk;
-    icon::k_window<<<grd, blk>>>(xy_d, 2, M, p->n0, p->b0, p->bf0, t.phix, kTaps, t.ix0);
-    icon::k_window<<<grd, blk>>>(xy_d + 1, 2, M, p->n1, p->b1, p->bf1, t.phiy, icon::kLdPhiy, t.iy0);
+    icon::k_window<<<grd, blk>>>(xy_d, 2, M, p->n0, p->b0, p->bf0, t.phix, kTaps, t.ix0, p->kb0, kb_inv(p->kb0));
+    icon::k_window<<<grd, blk>>>(xy_d + 1, 2, M, p->n1, p->b1, p->bf1, t.phiy, icon::kLdPhiy, t.iy0, p->kb1,
+                                 kb_inv(p->kb1));
     ICON_CUDA(cudaGetLastError());
     std::vector<int> ix0(M), iy0(M);
     ICON_CUDA(cudaMemcpy(ix0.data(), t.ix0, sizeof(int) * M, cudaMemcpyDeviceToHost));
     ICON_CUDA(cudaMemcpy(iy0.data(), t.iy0, sizeof(int) * M, cudaMemcpyDeviceToHost));
     // Entries (node j, x tap t0) grouped by grid row x = (ix0 + t0) mod n0,
-    // sorted within a row by (iy0, j).
-    const int n0 = p->n0;
+    // sorted within a row by (iy0, j); only the taps tlo..thi the window can
+    // make non-zero get entries.
+    const int n0 = p->n0, tlo = p->tlo, thi = p->thi;
+    t.taps = thi - tlo + 1;
     std::vector<int> cnt(n0 + 1, 0);
     for (int j = 0; j < M; ++j)
-        for (int t0 = 0; t0 < kTaps; ++t0) cnt[((ix0[j] + t0) % n0 + n0) % n0 + 1]++;
+        for (int t0 = tlo; t0 <= thi; ++t0) cnt[((ix0[j] + t0) % n0 + n0) % n0 + 1]++;
     for (int x = 0; x < n0; ++x) cnt[x + 1] += cnt[x];
     std::vector<int> pos(cnt.begin(), cnt.end() - 1);
-    size_t E = (size_t)M * kTaps;
+    size_t E = (size_t)M * t.taps;
     std::vector<int> jt(E), ky(E);
     for (int j = 0; j < M; ++j)
-        for (int t0 = 0; t0 < kTaps; ++t0) {
+        for (int t0 = tlo; t0 <= thi; ++t0) {
             int x = ((ix0[j] + t0) % n0 + n0) % n0;
             int e = pos[x]++;
             jt[e] = j * 16 + t0;
@@ -451,7 +488,7 @@ struct StageBytes {
 StageBytes stage_bytes(const icon_plan *p, const NodeTables &t)
 {
     StageBytes b;
-    double NN = (double)p->N0 * p->N1, G1 = (double)p->n0 * p->N1 * 8, MT = (double)t.M * kTaps, B = p->B;
+    double NN = (double)p->N0 * p->N1, G1 = (double)p->n0 * p->N1 * 8, MT = (double)t.M * t.taps, B = p->B;
     const double G1h = (double)(p->n0 / 2 + 1) * p->N1 * 8;   // rows 0..n0/2 (real image)
     b.xf_real = NN * 4 + G1h;
     b.xf_cplx = NN * 8 + G1;
@@ -830,6 +867,15 @@ static icon_status plan_create_impl(const icon_geometry *geo, int group, icon_pl
     p->M = nx * nz;
     grid_params(p->N0, p->th0, p->n0, p->b0, p->bf0);
     grid_params(p->N1, p->th1, p->n1, p->b1, p->bf1);
+    if (geo->window != ICON_WINDOW_GAUSS6 && geo->window != ICON_WINDOW_KB4)
+        return fail(ICON_ERR_INVALID, "window must be ICON_WINDOW_GAUSS6 or ICON_WINDOW_KB4");
+    p->window = geo->window;
+    if (p->window == ICON_WINDOW_KB4) {
+        p->kb0 = kb_shape(p->th0);
+        p->kb1 = kb_shape(p->th1);
+        p->tlo = icon::kKbTlo;
+        p->thi = icon::kKbThi;
+    }
     p->lg0 = ilog2(p->n0);
     p->lg1 = ilog2(p->n1);
     int nmax = std::max(p->n0, p->n1);
@@ -863,7 +909,7 @@ static icon_status plan_create_impl(const icon_geometry *geo, int group, icon_pl
     px2d(nx, nz, p->th_neg.data(), p->xy.data());
     weights(nx, nz, p->th_neg.data(), p->w.data());
     ICON_TRY(build_tables(p.get(), p->xy.data(), p->w.data(), p->M, p->nodes));
-    std::vector<float> cx = deapod(p->N0, p->n0, p->b0), cy = deapod(p->N1, p->n1, p->b1);
+    std::vector<float> cx = deapod(p->N0, p->n0, p->b0, p->kb0), cy = deapod(p->N1, p->n1, p->b1, p->kb1);
     ICON_TRY(p->arena.upload(&p->cx, cx.data(), cx.size()));
     ICON_TRY(p->arena.upload(&p->cy, cy.data(), cy.size()));
     std::vector<float> rcx(cx.size()), rcy(cy.size());
@@ -878,7 +924,8 @@ static icon_status plan_create_impl(const icon_geometry *geo, int group, icon_pl
     ICON_TRY(p->arena.upload(&px1_d, px1.data(), px1.size()));
     ICON_TRY(p->arena.alloc(&p->phi1, (size_t)nx * kTaps));
     ICON_TRY(p->arena.alloc(&p->i10, (size_t)nx));
-    icon::k_window<<<(nx + 255) / 256, 256>>>(px1_d, 1, nx, p->n0, p->b0, p->bf0, p->phi1, kTaps, p->i10);
+    icon::k_window<<<(nx + 255) / 256, 256>>>(px1_d, 1, nx, p->n0, p->b0, p->bf0, p->phi1, kTaps, p->i10, p->kb0,
+                                              kb_inv(p->kb0));
     ICON_CUDA(cudaGetLastError());
     std::vector<float2> t0 = twiddles(p->n0), t0h = twiddles(p->n0 / 2), t1 = twiddles(p->n1);
     ICON_TRY(p->arena.upload(&p->tw0, t0.data(), t0.size()));

@@ -48,7 +48,10 @@ void help()
            "    or its Toeplitz form, the exact operator as one convolution: faster, within 1e-4 of the default),\n"
            "  --tol T (end the ICON iterations of a batch once every slice's relative step is at most T; default 0,\n"
            "    the full -iter schedule), --resume (keep the slices whose reconstruction/mid%%05d.mrc already exists\n"
-           "    with this run's sizes; they are read back, not recomputed)\n");
+           "    with this run's sizes; they are read back, not recomputed),\n"
+           "  --window gauss6|kb4 (NUFFT window of the input stage, the reprojections and the NUFFT operator: the\n"
+           "    Gaussian of half-width 6, default, or the Kaiser-Bessel window of half-width 4, 8 taps instead of 14;\n"
+           "    the leave-one-out sweep of --loo keeps the Gaussian)\n");
 }
 
 struct Args {
@@ -65,6 +68,7 @@ struct Args {
     int op = ICON_OPERATOR_NUFFT;
     double tol = 0.0;
     bool resume = false;
+    int window = ICON_WINDOW_GAUSS6;
 };
 
 // Per-GPU work: a contiguous slice range.
@@ -162,7 +166,7 @@ void run_job(Job &job, const Args &A, const MrcHeader &inh, const std::vector<fl
     // Full reconstruction (Lib_2D2, MainCode.cu:3-177), in runs of slices
     // still to do (all of them unless --resume found finished ones).
     {
-        icon_geometry g{nx, thickness, nz, tilts.data(), cap, job.device};
+        icon_geometry g{nx, thickness, nz, tilts.data(), cap, job.device, A.window};
         icon_plan *plan = nullptr;
         if (icon_plan_create(&g, &plan) != ICON_OK) return fail("plan");
         struct Destroy {
@@ -234,7 +238,7 @@ void run_job(Job &job, const Args &A, const MrcHeader &inh, const std::vector<fl
     std::vector<float> t2;
     for (int i = 0; i < nz; ++i)
         if (i != omit) t2.push_back(tilts[i]);
-    icon_geometry g{nx, thickness, nz - 1, t2.data(), cap, job.device};
+    icon_geometry g{nx, thickness, nz - 1, t2.data(), cap, job.device, A.window};
     icon_plan *plan = nullptr;
     if (icon_plan_create(&g, &plan) != ICON_OK) return fail("cross-validation plan");
     if (icon_plan_set_reprojection(plan, tilts[omit]) != ICON_OK || icon_plan_set_operator(plan, A.op) != ICON_OK ||
@@ -279,6 +283,8 @@ int main(int argc, char **argv)
             else if (a == "--tol" && next_arg(argc, argv, i, v)) A.tol = std::max(0.0, atof(v.c_str()));
             else if (a == "--operator" && next_arg(argc, argv, i, v) && (v == "nufft" || v == "toeplitz"))
                 A.op = v == "toeplitz" ? ICON_OPERATOR_TOEPLITZ : ICON_OPERATOR_NUFFT;
+            else if (a == "--window" && next_arg(argc, argv, i, v) && (v == "gauss6" || v == "kb4"))
+                A.window = v == "kb4" ? ICON_WINDOW_KB4 : ICON_WINDOW_GAUSS6;
             else if (a == "--help") { help(); return -1; }
             else { printf("parameter error!\n Please use -help to see the manual\n"); return -1; }
             continue;

@@ -15,6 +15,8 @@ namespace icon {
 
 constexpr int kTaps = 14;   // 2m+2 taps per dimension, m = 6 (nufft_gpu_v8.cuh:5, NU:226)
 constexpr int kHalf = 6;    // window half-width m
+constexpr int kKbHalf = 4;  // half-width K of the Kaiser-Bessel window (taps 3..10 of the 14)
+constexpr int kKbTlo = kHalf - kKbHalf + 1, kKbThi = kHalf + kKbHalf;
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {

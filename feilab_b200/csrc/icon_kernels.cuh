@@ -40,6 +40,7 @@ constexpr int kLdPhiy = 16;   // phiy rows padded to 16 floats (four 16-byte loa
 // Device view of one tilt-series geometry (all pointers are device memory).
 struct Geo {
     int N0, N1, n0, n1, lg0, lg1, M, nx, nz, B;
+    int tlo, thi;          // taps that can be non-zero: 0..13 (Gaussian), 3..10 (Kaiser-Bessel)
     const float *w;        // [M] density weights (Weight, weight.cu:8-41), group g's at w + g*wstride
     size_t wstride;        // 0: one weight vector for every group; M: one per group
     const float *phix;     // [M][14] window values, x taps   (NU:221-235)
@@ -73,9 +74,13 @@ struct Geo1 {
 // ------------------------------------------------------------- tables ----
 // Window taps exactly as nufft_Phi2d_1dCU (NU:221-235) computes them, in float:
 // l = floor(n*x) - m + t, x1 = x - l/n, phi = bf*exp(-(n*x1)^2/b).  Rows of
-// ld >= 14 floats, the pad zeroed.
+// ld >= 14 floats, the pad zeroed.  kb > 0 selects the Kaiser-Bessel window
+// of half-width kKbHalf in the same taps (non-zero on taps 3..10 only): with
+// u = n*x1 (exact in float, n a power of two),
+// phi = sinh(kb sqrt(K^2 - u^2)) / sqrt(K^2 - u^2) * inv for |u| < K, else 0,
+// evaluated in double and rounded once (inv = 1/(pi I0(kb K))).
 __global__ void k_window(const float *__restrict__ x, int stride, int M, int n, float b, float bf,
-                         float *__restrict__ phi, int ld, int *__restrict__ l0out)
+                         float *__restrict__ phi, int ld, int *__restrict__ l0out, double kb, double inv)
 {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= M) return;
@@ -86,7 +91,13 @@ __global__ void k_window(const float *__restrict__ x, int stride, int M, int n, 
     for (int t = 0; t < kTaps; ++t) {
         int l = l0 + t;
         float x1 = xv - (float)l / (float)n;
-        phi[(size_t)j * ld + t] = bf * expf(-((n * x1) * (n * x1) / b));
+        if (kb > 0.0) {
+            const double u = (double)(n * x1);
+            const double q = (double)(kKbHalf * kKbHalf) - u * u;
+            phi[(size_t)j * ld + t] = q > 0.0 ? (float)(sinh(kb * sqrt(q)) / sqrt(q) * inv) : 0.f;
+        } else {
+            phi[(size_t)j * ld + t] = bf * expf(-((n * x1) * (n * x1) / b));
+        }
     }
     for (int t = kTaps; t < ld; ++t) phi[(size_t)j * ld + t] = 0.f;
 }
@@ -404,6 +415,7 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
             for (int k = 0; k < 4; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
             for (int pr = 0; pr < kTaps / 2; ++pr) {
+                if (2 * pr + 1 < g.tlo || 2 * pr > g.thi) continue;   // both taps zero (Kaiser-Bessel)
                 const float wa = py[2 * pr], wb = py[2 * pr + 1];
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
@@ -429,6 +441,7 @@ __global__ void FFT_BOUNDS(E) k_ypass_fwd(Geo g, const float2 *__restrict__ G1, 
             for (int b = 0; b < B; ++b) acc[b] = make_float2(0.f, 0.f);
 #pragma unroll
             for (int t1 = 0; t1 < kTaps; ++t1) {
+                if (t1 < g.tlo || t1 > g.thi) continue;   // zero tap (Kaiser-Bessel)
                 float2 v[B];
                 load_b<B>(sr + t1 * SB, v);
 #pragma unroll
@@ -468,6 +481,7 @@ __global__ void k_interp_fin(Geo g, const float2 *__restrict__ P, float2 *__rest
         float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
         for (int t0 = 0; t0 < kTaps; ++t0) {
+            if (t0 < g.tlo || t0 > g.thi) continue;   // taps without entries (Kaiser-Bessel)
             float2 v = pp[(size_t)t0 * B];
             float p = __ldg(&px[t0]);
             acc.x = fmaf(v.x, p, acc.x);
@@ -552,12 +566,15 @@ __host__ __device__ inline size_t ypass_adj_smem(int n1, int B)
 // table (last index lbmax) and off the index of the chunk's first entry.
 template <int B, int SB, int R>
 __device__ __forceinline__ void gather_rows(int i0, int r0ofs, const unsigned short *lb, int lbmax, int off, int cn,
-                                            const float2 *Qs, const float *Ps, const int *Rs, float2 (&acc)[R][B])
+                                            const float2 *Qs, const float *Ps, const int *Rs, float2 (&acc)[R][B],
+                                            int tlo, int thi)
 {
     // lb[lbmax] counts every entry of the row, so clamping an index past it
-    // (alias ranges of wide thread strips) is exact.
-    int lo = min(max((int)lb[min(max(i0 - (kTaps - 1), 0), lbmax)] - off, 0), cn);
-    int hi = min(max((int)lb[min(max(i0 + R, 0), lbmax)] - off, 0), cn);
+    // (alias ranges of wide thread strips) is exact.  Only taps tlo..thi of a
+    // window can be non-zero, so the entries with r0 in [i0 - thi, i0 + R - 1 - tlo]
+    // are the ones that reach these rows.
+    int lo = min(max((int)lb[min(max(i0 - thi, 0), lbmax)] - off, 0), cn);
+    int hi = min(max((int)lb[min(max(i0 + R - tlo, 0), lbmax)] - off, 0), cn);
     const int iu = i0 - r0ofs;
     for (int e = lo; e < hi; ++e) {
         const int t0 = iu - Rs[e];        // tap of row i0; row i0 + k uses t0 + k
@@ -666,11 +683,13 @@ __global__ void FFT_BOUNDS(E) k_ypass_adj(Geo g, const float2 *__restrict__ f, f
         for (int k = 0; k < NS; ++k) {
             const int r = RS * (threadIdx.x + k * T);
             if (r < n) {
-                gather_rows<B, SB, RS>(r + kHalo, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
+                gather_rows<B, SB, RS>(r + kHalo, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k], g.tlo, g.thi);
                 // Rows 0..7 and n-8..n-1 also take the halo rows that alias
                 // them (kHalo is a multiple of RS, so no strip straddles).
-                if (r < kHalo) gather_rows<B, SB, RS>(r + kHalo + n, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
-                if (r >= n - kHalo) gather_rows<B, SB, RS>(r + kHalo - n, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k]);
+                if (r < kHalo)
+                    gather_rows<B, SB, RS>(r + kHalo + n, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k], g.tlo, g.thi);
+                if (r >= n - kHalo)
+                    gather_rows<B, SB, RS>(r + kHalo - n, r0ofs, lb, ldl - 1, off, cn, Qs, Ps, Rs, acc[k], g.tlo, g.thi);
             }
         }
     }

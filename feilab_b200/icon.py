@@ -43,6 +43,8 @@ def lib():
         L.icon_rows_forward.argtypes = [P, V, V, I, V]
         L.icon_prepare_rhs.argtypes = [P, V, V, I, V]
         L.icon_solve.argtypes = [P, ctypes.POINTER(SolveCfg), V, V, I, I, V, V, V]
+        L.icon_solve_warm.argtypes = [P, ctypes.POINTER(SolveCfg), V, V, I, ctypes.POINTER(WarmCfg), V,
+                                      ctypes.POINTER(I), V]
         L.icon_solve_until.argtypes = [P, ctypes.POINTER(SolveCfg), V, V, I, I, ctypes.c_double, I,
                                        ctypes.POINTER(I), V, V]
         L.icon_reproject.argtypes = [P, V, F, V, I, V]
@@ -70,7 +72,7 @@ def lib():
         L.icon_last_error.restype = ctypes.c_char_p
         for name in ("icon_plan_create", "icon_plan_destroy", "icon_plan_query", "icon_plan_geometry",
                      "icon_nufft_forward", "icon_nufft_forward_complex", "icon_nufft_adjoint",
-                     "icon_rows_forward", "icon_prepare_rhs", "icon_solve", "icon_solve_until", "icon_reproject",
+                     "icon_rows_forward", "icon_prepare_rhs", "icon_solve", "icon_solve_until", "icon_solve_warm", "icon_reproject",
                      "icon_reconstruct_host", "icon_trace_enable", "icon_trace_read", "icon_prepare_rhs_stack",
                      "icon_reconstruct_stack", "icon_reconstruct_stack_host", "icon_host_alloc", "icon_host_free",
                      "icon_stack_upload", "icon_device_free", "icon_weights", "icon_plan_set_group_weights",
@@ -89,7 +91,21 @@ OUT_SLICES, OUT_REPROJECTION = 1, 2
 
 class Geometry(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("thickness", ctypes.c_int), ("ntilt", ctypes.c_int),
-                ("tilt_deg", ctypes.POINTER(ctypes.c_float)), ("capacity", ctypes.c_int), ("device", ctypes.c_int)]
+                ("tilt_deg", ctypes.POINTER(ctypes.c_float)), ("capacity", ctypes.c_int), ("device", ctypes.c_int),
+                ("window", ctypes.c_int)]
+
+
+# NUFFT windows (ICON_WINDOW_*): the reference's Gaussian (half-width 6, 14
+# taps) and the Kaiser-Bessel window of half-width 4 (8 taps).
+WINDOWS = {"gauss6": 0, "kb4": 1}
+
+
+class WarmCfg(ctypes.Structure):
+    _fields_ = [("tol", ctypes.c_double), ("check_every", ctypes.c_int), ("max_dist", ctypes.c_double)]
+
+
+# Per-slice outcome of IconPlan.solve_warm (ICON_WARM_*).
+WARM_OUTCOMES = {0: "accepted", 1: "not finite", 2: "not converged", 3: "too far from the cold INFR iterate"}
 
 
 class SolveCfg(ctypes.Structure):
@@ -115,16 +131,18 @@ def _ptr(t):
 class IconPlan:
     """Plan for one tilt series: nx detector pixels, `thickness` (0 = nx)
     reconstruction rows, tilt angles as in the .tlt file, up to `capacity`
-    slices per call."""
+    slices per call; window "gauss6" (the reference's) or "kb4"."""
 
-    def __init__(self, nx, thickness, tilts, capacity=8, device=None):
+    def __init__(self, nx, thickness, tilts, capacity=8, device=None, window="gauss6"):
         import torch
         if device is None:
             device = torch.cuda.current_device()
         self.device = torch.device("cuda", device)
         self.tilts = np.ascontiguousarray(np.asarray(tilts, np.float32))
         g = Geometry(int(nx), int(thickness), len(self.tilts),
-                     self.tilts.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(capacity), int(device))
+                     self.tilts.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(capacity), int(device),
+                     WINDOWS[window])
+        self.window = window
         h = ctypes.c_void_p()
         self._destroy = lib().icon_plan_destroy     # held so that __del__ works at interpreter exit
         _check(lib().icon_plan_create(ctypes.byref(g), ctypes.byref(h)))
@@ -258,6 +276,24 @@ class IconPlan:
                                       warm, float(tol), int(check_every), ctypes.byref(n),
                                       step.ctypes.data_as(ctypes.c_void_p), _stream()))
         return m, int(n.value), step
+
+    def solve_warm(self, Ahwb, m0, tol, iters=(0, 10, 0), data_type=1, threshold=0.03, check_every=10, max_dist=1.0):
+        """Warm-started solve from m0 with the cold start as judge and
+        fallback (icon_solve_warm): returns (m, per-slice outcome codes
+        ICON_WARM_* as an int array, 0 = accepted, else redone from m = 0,
+        iterations of the warm solve)."""
+        import torch
+        S = Ahwb.shape[0]
+        a, b, c = iters
+        cfg = SolveCfg(int(a), int(b), int(c), int(data_type), float(threshold))
+        wc = WarmCfg(float(tol), int(check_every), float(max_dist))
+        m = self._dev(m0, torch.float32).clone()
+        redone = np.zeros(S, np.int32)
+        n = ctypes.c_int(0)
+        _check(lib().icon_solve_warm(self._h, ctypes.byref(cfg), _ptr(self._dev(Ahwb, torch.complex64)), _ptr(m), S,
+                                     ctypes.byref(wc), redone.ctypes.data_as(ctypes.c_void_p), ctypes.byref(n),
+                                     _stream()))
+        return m, redone, int(n.value)
 
     def reproject(self, m, tilt_deg=None):
         """m (S, N0, N1) float32 -> (S, nx) float32 reprojection at tilt_deg

@@ -60,7 +60,25 @@ typedef struct {
                                 negated internally as MainCode.cu:42 does          */
     int capacity;            /* most slices any single call will pass            */
     int device;              /* CUDA device ordinal; -1 = the current device     */
+    int window;              /* NUFFT window: ICON_WINDOW_GAUSS6 (0, the
+                                reference's) or ICON_WINDOW_KB4                  */
 } icon_geometry;
+
+/* NUFFT windows.  ICON_WINDOW_GAUSS6 is the reference's Gaussian of
+ * half-width m = 6 with 2m+2 = 14 taps per dimension (NU:221-235,
+ * NU:471-476) and deapodisation exp(-b (pi k/n)^2) (NU:22-42): the parity
+ * mode.  ICON_WINDOW_KB4 (no counterpart in the reference) is the
+ * Kaiser-Bessel window of half-width K = 4 grid points, 8 taps per
+ * dimension: phi(u) = sinh(kb sqrt(K^2 - u^2)) / (pi sqrt(K^2 - u^2)) for
+ * |u| < K (u in grid units), kb = pi (2 - 1/theta), deapodisation
+ * I0(K sqrt(kb^2 - (2 pi k/n)^2)), both scaled by 1/I0(kb K).  It
+ * approximates the non-uniform DFT about four times more closely than the
+ * Gaussian (1.5e-7 against 6.4e-7 relative in float at 64x40) and the
+ * y-passes gather 8 x 8 instead of 14 x 14 taps per node.  The
+ * iterations' Toeplitz operator has no window, so the window changes only
+ * the NUFFT stages (input stage, reprojection, the NUFFT operator). */
+#define ICON_WINDOW_GAUSS6 0
+#define ICON_WINDOW_KB4 1
 
 /* Iteration schedule and constraint of Iteration3 (Iteration2.cu:3-150):
  * `infr_before` unconstrained steps, `icon` clamped steps, `infr_after`
@@ -239,6 +257,40 @@ icon_status icon_solve(icon_plan *plan, const icon_solve_cfg *cfg, const void *d
  * such stop: it always runs the full count. */
 icon_status icon_solve_until(icon_plan *plan, const icon_solve_cfg *cfg, const void *d_Ahwb, float *d_m, int S,
                              int warm_start, double tol, int check_every, int *h_iters, double *h_step, void *stream);
+
+/* Acceptance test of a warm-started solve (icon_solve_warm). */
+typedef struct {
+    double tol;          /* relative-step tolerance of the ICON phase (> 0), as icon_solve_until */
+    int check_every;     /* ICON iterations between checks (>= 1)                               */
+    double max_dist;     /* largest accepted ||m - m_infr|| / ||m_infr|| (> 0), m_infr the cold
+                            start's iterate after the first INFR phase                           */
+} icon_warm_cfg;
+
+/* Reasons icon_solve_warm redid a slice from m = 0 (h_redone[s]). */
+#define ICON_WARM_ACCEPTED 0
+#define ICON_WARM_NOT_FINITE 1      /* the warm result holds a NaN or an infinity       */
+#define ICON_WARM_NOT_CONVERGED 2   /* its relative step stayed above tol               */
+#define ICON_WARM_TOO_FAR 3         /* farther than max_dist from the cold INFR iterate */
+
+/* Warm-started solve with the plain cold-start solve as fallback.  d_m
+ * [S][N0][N1] holds each slice's start on entry (e.g. icon_ws_predict's
+ * output) and its result on return.  The schedule runs from those starts
+ * with the ICON phase stopped at wc->tol (icon_solve_until).  The cold
+ * start's first INFR phase (cfg->infr_before iterations from m = 0, a few
+ * percent of the schedule) gives m_infr.  A slice is accepted when its
+ * result is finite, its last relative step is at most tol, and
+ * ||m - m_infr|| <= max_dist ||m_infr||; every other slice is solved again
+ * from m = 0 with the full schedule (icon_solve with warm_start = 0) and its
+ * result replaced by that cold one, which is bit for bit what icon_solve
+ * gives for the slice (slices do not interact).  h_redone[S] (optional)
+ * receives ICON_WARM_* per slice, *h_iters (optional) the iterations of the
+ * warm solve.  Allocates device scratch for the slices it redoes;
+ * synchronises the stream.  The redone slices run as slices 0.. of a new
+ * batch, so a plan with per-group weights (icon_plan_set_group_weights)
+ * would solve them with other groups' weights: use one without.  No counterpart in the reference, which always
+ * starts from m = 0 (Iteration2.cu:33). */
+icon_status icon_solve_warm(icon_plan *plan, const icon_solve_cfg *cfg, const void *d_Ahwb, float *d_m, int S,
+                            const icon_warm_cfg *wc, int *h_redone, int *h_iters, void *stream);
 
 /* Reprojection of S solved slices at one tilt angle (given as in the .tlt
  * file): forward 2-D NUFFT at the nodes of that single tilt, then the 1-D

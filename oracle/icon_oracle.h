@@ -30,6 +30,12 @@ extern "C" {
 #define ORA_M 6
 /* Taps per dimension, 2m+2 (NU:226). */
 #define ORA_T 14
+/* Window kinds: the reference's Gaussian of half-width 6, and a Kaiser-Bessel
+ * window of half-width 4 (no counterpart in the reference) laid out in the
+ * same 14 taps, non-zero on taps 3..10 only. */
+#define ORA_WINDOW_GAUSS6 0
+#define ORA_WINDOW_KB4 1
+#define ORA_KB_M 4
 
 /* Grid parameters for one dimension of size N: theta = 2*2^ceil(log2 N)/N as
  * float, n = ceil(theta*N), window b and bf (MainCode.cu:66-71, NU:471-476). */

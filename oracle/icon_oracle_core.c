@@ -40,6 +40,8 @@ static inline REAL madd(REAL a, REAL b, REAL acc)
 typedef struct {
     int nx, nz, N0, N1, n0, n1, M;
     float th0, th1, b0, bf0, b1, bf1;
+    int window;         /* ORA_WINDOW_GAUSS6 (the reference's) or ORA_WINDOW_KB4 */
+    double kb0, kb1;    /* Kaiser-Bessel shape b = pi (2 - 1/theta) per dimension */
     float *xy;          /* [M][2] node coordinates (px2D)          */
     float *w;           /* [M] density weights (Weight)            */
     REAL *phix, *phiy;  /* [M][14] window values per tap           */
@@ -131,16 +133,48 @@ static void fft2(const ora_plan *p, REAL *g, int inverse, REAL *col)
 }
 
 /* ------------------------------------------------------------ windows ---- */
+/* Modified Bessel function I0 by its power series sum_k ((x/2)^k / k!)^2, in
+ * double (all terms positive; 60 terms are far more than x <= 40 needs). */
+static double bessel_i0(double x)
+{
+    double term = 1.0, sum = 1.0, q = 0.25 * x * x;
+    for (int k = 1; k < 60; k++) {
+        term *= q / ((double)k * (double)k);
+        sum += term;
+        if (term < 1e-18 * sum) break;
+    }
+    return sum;
+}
+
 /* NU:221-235 (nufft_Phi2d_1dCU) and NU:1242-1256 (nufft_Phi1dCU):
  * l = floor(n*x) - m + t, x1 = x - l/n, phi = bf*exp(-(n*x1)^2/b),
- * index (l+n) % n.  The float build repeats the float expression with expf. */
-static void window_taps(float x, int n, float b, float bf, REAL *phi, int *idx)
+ * index (l+n) % n.  The float build repeats the float expression with expf.
+ *
+ * ORA_WINDOW_KB4 (no counterpart in the reference): the Kaiser-Bessel window
+ * of half-width K = 4 grid points in the same 14-tap layout, u = n*x1,
+ *   phi(u) = sinh(kb sqrt(K^2 - u^2)) / (pi sqrt(K^2 - u^2)) / I0(kb K)  for |u| < K,
+ * 0 otherwise (so only taps 3..10 can be non-zero), kb = pi (2 - 1/theta)
+ * (Kaiser 1974; Jackson et al., IEEE TMI 10 (1991); the shape parameter of
+ * Potts, Steidl and Tasche's NFFT).  Its Fourier transform, the
+ * deapodisation below, is I0(K sqrt(kb^2 - (2 pi k / n)^2)) / I0(kb K). */
+static void window_taps(float x, int n, float b, float bf, int kind, double kb, REAL *phi, int *idx)
 {
     float nf = (float)n * x;
     int l0 = (int)(floorf(nf) - ORA_M);
+    const double inv = 1.0 / (REF_PI * bessel_i0(kb * ORA_KB_M));
     for (int t = 0; t < ORA_T; t++) {
         int l = l0 + t;
-        if (IS_F32) {
+        if (kind == ORA_WINDOW_KB4) {
+            /* u = n*x1 is exact in float (n is a power of two); the window
+             * itself is evaluated in double in both builds and rounded once,
+             * since sinh of arguments up to kb*K ~ 19 would amplify float
+             * rounding of its argument ~19-fold. */
+            float x1f = x - (float)l / (float)n;
+            double u = IS_F32 ? (double)((float)n * x1f) : (double)n * ((double)x - (double)l / (double)n);
+            double q = (double)(ORA_KB_M * ORA_KB_M) - u * u;
+            double v = q > 0.0 ? sinh(kb * sqrt(q)) / sqrt(q) * inv : 0.0;
+            phi[t] = IS_F32 ? (REAL)(float)v : (REAL)v;
+        } else if (IS_F32) {
             float x1 = x - (float)l / (float)n;
             float q = ((float)n * x1) * ((float)n * x1) / b;
             phi[t] = (REAL)(bf * expf(-q));
@@ -155,12 +189,21 @@ static void window_taps(float x, int n, float b, float bf, REAL *phi, int *idx)
 
 /* NU:22-42 (nufft_ck2d2) and NU:1258-1271 (nufft_ck1d): per-dimension
  * deapodisation exp(-b (pi k / n)^2), k = X - N/2, evaluated in double; the
- * reference stores each factor as float and multiplies the two in float. */
-static void deapod(int N, int n, float b, REAL *c)
+ * reference stores each factor as float and multiplies the two in float.
+ * Kaiser-Bessel: I0(K sqrt(kb^2 - (2 pi k/n)^2)) / I0(kb K) (kb >= pi/theta
+ * >= 2 pi |k|/n for theta >= 1, so the root is real). */
+static void deapod(int N, int n, float b, int kind, double kb, REAL *c)
 {
+    const double i0m = bessel_i0(kb * ORA_KB_M);
     for (int X = 0; X < N; X++) {
         int k = X - N / 2;
-        double v = exp(-(double)b * ((REF_PI * k / (double)n) * (REF_PI * k / (double)n)));
+        double v;
+        if (kind == ORA_WINDOW_KB4) {
+            double w = 2.0 * REF_PI * k / (double)n;
+            v = bessel_i0(ORA_KB_M * sqrt(kb * kb - w * w)) / i0m;
+        } else {
+            v = exp(-(double)b * ((REF_PI * k / (double)n) * (REF_PI * k / (double)n)));
+        }
         c[X] = IS_F32 ? (REAL)(float)v : (REAL)v;
     }
 }
@@ -168,10 +211,12 @@ static void deapod(int N, int n, float b, REAL *c)
 /* -------------------------------------------------------------- plans ---- */
 /* Builds what Lib_2D2 builds for one tilt series (MainCode.cu:38-109):
  * negated angles, nodes, weights, grid sizes, window tables, deapodisation. */
-int FN(ora_plan_create)(int nx, int thickness, int nz, const float *tlt, void **out)
+int FN(ora_plan_create_w)(int nx, int thickness, int nz, const float *tlt, int window, void **out)
 {
     if (nx < 8 || thickness < 8 || nz < 2 || !tlt || !out) return 1;
+    if (window != ORA_WINDOW_GAUSS6 && window != ORA_WINDOW_KB4) return 1;
     ora_plan *p = (ora_plan *)calloc(1, sizeof(ora_plan));
+    p->window = window;
     p->nx = nx;
     p->nz = nz;
     p->N0 = nx;
@@ -179,6 +224,8 @@ int FN(ora_plan_create)(int nx, int thickness, int nz, const float *tlt, void **
     p->M = nx * nz;
     ora_grid_params(p->N0, &p->th0, &p->n0, &p->b0, &p->bf0);
     ora_grid_params(p->N1, &p->th1, &p->n1, &p->b1, &p->bf1);
+    p->kb0 = REF_PI * (2.0 - 1.0 / (double)p->th0);
+    p->kb1 = REF_PI * (2.0 - 1.0 / (double)p->th1);
     float *th = (float *)malloc(sizeof(float) * (size_t)nz);
     for (int i = 0; i < nz; i++) th[i] = -tlt[i];       /* MainCode.cu:42 */
     p->xy = (float *)malloc(sizeof(float) * 2 * (size_t)p->M);
@@ -192,19 +239,21 @@ int FN(ora_plan_create)(int nx, int thickness, int nz, const float *tlt, void **
     p->ix = (int *)malloc(sizeof(int) * MT);
     p->iy = (int *)malloc(sizeof(int) * MT);
     for (int j = 0; j < p->M; j++) {
-        window_taps(p->xy[2 * j], p->n0, p->b0, p->bf0, p->phix + (size_t)j * ORA_T, p->ix + (size_t)j * ORA_T);
-        window_taps(p->xy[2 * j + 1], p->n1, p->b1, p->bf1, p->phiy + (size_t)j * ORA_T, p->iy + (size_t)j * ORA_T);
+        window_taps(p->xy[2 * j], p->n0, p->b0, p->bf0, window, p->kb0, p->phix + (size_t)j * ORA_T,
+                    p->ix + (size_t)j * ORA_T);
+        window_taps(p->xy[2 * j + 1], p->n1, p->b1, p->bf1, window, p->kb1, p->phiy + (size_t)j * ORA_T,
+                    p->iy + (size_t)j * ORA_T);
     }
     p->cx = (REAL *)malloc(sizeof(REAL) * (size_t)p->N0);
     p->cy = (REAL *)malloc(sizeof(REAL) * (size_t)p->N1);
-    deapod(p->N0, p->n0, p->b0, p->cx);
-    deapod(p->N1, p->n1, p->b1, p->cy);
+    deapod(p->N0, p->n0, p->b0, window, p->kb0, p->cx);
+    deapod(p->N1, p->n1, p->b1, window, p->kb1, p->cy);
     /* 1-D row transform: nodes (k - nx/2)/nx on the n0 grid (MainCode.cu:72-80). */
     p->phi1 = (REAL *)malloc(sizeof(REAL) * (size_t)nx * ORA_T);
     p->i1 = (int *)malloc(sizeof(int) * (size_t)nx * ORA_T);
     for (int k = 0; k < nx; k++) {
         float x = (float)(((double)(float)k - (double)(float)nx / 2.0) / (double)(float)nx);
-        window_taps(x, p->n0, p->b0, p->bf0, p->phi1 + (size_t)k * ORA_T, p->i1 + (size_t)k * ORA_T);
+        window_taps(x, p->n0, p->b0, p->bf0, window, p->kb0, p->phi1 + (size_t)k * ORA_T, p->i1 + (size_t)k * ORA_T);
     }
     p->tw0 = make_twiddles(p->n0);
     p->tw1 = make_twiddles(p->n1);
@@ -216,17 +265,27 @@ int FN(ora_plan_create)(int nx, int thickness, int nz, const float *tlt, void **
 
 /* A plan whose nodes are one line at a single angle (the reprojection plan of
  * MainCode.cu:101-109), sharing grid parameters with a series of width nx. */
-int FN(ora_plan_create_line)(int nx, int thickness, float angle_neg, void **out)
+int FN(ora_plan_create)(int nx, int thickness, int nz, const float *tlt, void **out)
+{
+    return FN(ora_plan_create_w)(nx, thickness, nz, tlt, ORA_WINDOW_GAUSS6, out);
+}
+
+int FN(ora_plan_create_line_w)(int nx, int thickness, float angle_neg, int window, void **out)
 {
     float t2[2] = {-angle_neg, -angle_neg};
     void *pp;
-    int rc = FN(ora_plan_create)(nx, thickness, 2, t2, &pp);
+    int rc = FN(ora_plan_create_w)(nx, thickness, 2, t2, window, &pp);
     if (rc) return rc;
     ora_plan *p = (ora_plan *)pp;
     p->nz = 1;
     p->M = nx;
     *out = p;
     return 0;
+}
+
+int FN(ora_plan_create_line)(int nx, int thickness, float angle_neg, void **out)
+{
+    return FN(ora_plan_create_line_w)(nx, thickness, angle_neg, ORA_WINDOW_GAUSS6, out);
 }
 
 void FN(ora_plan_destroy)(void *pp)

@@ -48,6 +48,8 @@ def _declare(L):
     for sfx in ("_f64", "_f32"):
         getattr(L, "ora_plan_create" + sfx).argtypes = [_I, _I, _I, fp, ctypes.POINTER(_P)]
         getattr(L, "ora_plan_create_line" + sfx).argtypes = [_I, _I, _F, ctypes.POINTER(_P)]
+        getattr(L, "ora_plan_create_w" + sfx).argtypes = [_I, _I, _I, fp, _I, ctypes.POINTER(_P)]
+        getattr(L, "ora_plan_create_line_w" + sfx).argtypes = [_I, _I, _F, _I, ctypes.POINTER(_P)]
         getattr(L, "ora_plan_destroy" + sfx).argtypes = [_P]
         getattr(L, "ora_plan_dims" + sfx).argtypes = [_P, ctypes.POINTER(_I)]
         getattr(L, "ora_plan_geometry" + sfx).argtypes = [_P, _P, _P, _P]
@@ -87,20 +89,28 @@ class OraclePlan:
     """One tilt series (nx, thickness, tilt angles as read from the .tlt file).
 
     precision: "f64" (the FP64 oracle) or "f32" (float rounding as the
-    reference, radix-2 FFT in place of cuFFT).
+    reference, radix-2 FFT in place of cuFFT).  window: "gauss6" (the
+    reference's Gaussian window) or "kb4" (Kaiser-Bessel, half-width 4).
     """
 
-    def __init__(self, nx: int, thickness: int, tilts, precision: str = "f64", line_angle=None):
+    WINDOWS = {"gauss6": 0, "kb4": 1}
+
+    def __init__(self, nx: int, thickness: int, tilts, precision: str = "f64", line_angle=None, window="gauss6"):
         self.sfx = "_" + precision
         self.real = np.float64 if precision == "f64" else np.float32
         self.cplx = np.complex128 if precision == "f64" else np.complex64
         h = ctypes.c_void_p()
         L = lib()
+        wk = self.WINDOWS[window]
+        self.window = window
         if line_angle is not None:
-            rc = getattr(L, "ora_plan_create_line" + self.sfx)(nx, thickness, ctypes.c_float(line_angle), ctypes.byref(h))
+            rc = getattr(L, "ora_plan_create_line_w" + self.sfx)(nx, thickness, ctypes.c_float(line_angle), wk,
+                                                                 ctypes.byref(h))
         else:
             t = np.ascontiguousarray(np.asarray(tilts, dtype=np.float32))
-            rc = getattr(L, "ora_plan_create" + self.sfx)(nx, thickness, len(t), t.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(h))
+            rc = getattr(L, "ora_plan_create_w" + self.sfx)(nx, thickness, len(t),
+                                                            t.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), wk,
+                                                            ctypes.byref(h))
         if rc != 0:
             raise ValueError(f"oracle plan rejected (nx={nx}, thickness={thickness})")
         self._h = h

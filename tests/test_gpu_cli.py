@@ -208,3 +208,29 @@ def test_cli_toeplitz_operator_and_tolerance(golden, tmp_path):
         assert 0 < rel_l2(dl[0], d[0]) < 0.5, s
     p = _run(base + ["-skipCV", "1", "--operator", "other"], str(tmp_path))
     assert p.returncode != 0 and "parameter error!" in p.stdout
+
+
+@pytest.mark.gpu
+def test_cli_kaiser_bessel_window(golden, tmp_path):
+    # --window kb4 reconstructs within the parity bar of the default
+    # (Gaussian) run, cross-validation files included; an unknown window is
+    # a parameter error.
+    from feilab_b200 import mrc
+    sched = (1, 40, 1)
+    z, out, base = _cli_case(golden, tmp_path, "gauss", sched)
+    S = int(z["S"])
+    assert _run(base, str(tmp_path)).returncode == 0
+    _, out_k, base_k = _cli_case(golden, tmp_path, "kb", sched)
+    p = _run(base_k + ["--window", "kb4"], str(tmp_path))
+    assert p.returncode == 0, p.stdout + p.stderr
+    for s in range(S):
+        _, d = mrc.read(str(out / "reconstruction" / f"mid{s:05d}.mrc"))
+        _, dk = mrc.read(str(out_k / "reconstruction" / f"mid{s:05d}.mrc"))
+        assert d.shape == dk.shape
+        assert rel_l2(dk[0], d[0]) < TOL_SOLVE, s
+    for n in ("fullRec_reProjection.mrc", "crossV_reprojection.mrc"):
+        _, r = mrc.read(str(out / "crossValidation" / n))
+        _, rk = mrc.read(str(out_k / "crossValidation" / n))
+        assert rel_l2(rk, r) < TOL_SOLVE, n
+    p = _run(base + ["-skipCV", "1", "--window", "kb6"], str(tmp_path))
+    assert p.returncode != 0 and "parameter error!" in p.stdout

@@ -34,6 +34,28 @@ def test_nufft_vs_direct_ndft(prec):
     assert rel_l2(p.adjoint(f), p.ndft_adjoint(f)) < 5e-6
 
 
+@pytest.mark.parametrize("prec,bound", [("f64", 2e-7), ("f32", 4e-7)])
+def test_kaiser_bessel_window_vs_direct_ndft(prec, bound):
+    """The Kaiser-Bessel mode (half-width 4, no counterpart in the
+    reference): non-zero on taps 3..10 of the 14 only, and closer to the
+    direct NDFT than the reference's Gaussian of half-width 6."""
+    tilts = np.arange(-60, 61, 3).astype(np.float32)
+    rng = np.random.default_rng(3)
+    for nx, th in ((64, 40), (50, 37), (128, 96)):
+        kb = OraclePlan(nx, th, tilts, prec, window="kb4")
+        ga = OraclePlan(nx, th, tilts, prec)
+        phix, _, phiy, _, cx, cy = kb.windows()
+        assert not np.any(phix[:, :3]) and not np.any(phix[:, 11:]), (nx, th)
+        assert not np.any(phiy[:, :3]) and not np.any(phiy[:, 11:]), (nx, th)
+        assert np.all(cx > 0) and np.all(cy > 0)
+        img = rng.standard_normal((nx, th))
+        f = rng.standard_normal(kb.M) + 1j * rng.standard_normal(kb.M)
+        e_kb = max(rel_l2(kb.forward(img), kb.ndft_forward(img)), rel_l2(kb.adjoint(f), kb.ndft_adjoint(f)))
+        e_ga = max(rel_l2(ga.forward(img), ga.ndft_forward(img)), rel_l2(ga.adjoint(f), ga.ndft_adjoint(f)))
+        assert e_kb < bound, (nx, th, e_kb)
+        assert e_kb < e_ga, (nx, th, e_kb, e_ga)
+
+
 def test_adjoint_identity_fp64():
     tilts = np.linspace(-58, 61, 17).astype(np.float32)
     p = OraclePlan(33, 21, tilts, "f64")
