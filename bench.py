@@ -84,14 +84,30 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def bf16_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return {"peak_tflops": float(json.load(open(p))["bf16_tflops"]), "peak_source": "measured (cuBLAS bf16 burst)"}
+    return {"peak_tflops": 1590.0, "peak_source": "fallback"}
+
+
+# Traced kernel kind -> (committed ncu summary, line holding its per-slot DRAM bytes).
+PROFILE_LINES = {"ypass_toep": ("ypass_toep_cfg2.txt", "dram_bytes_per_slot"),
+                 "ypass_toep_quad": ("ypass_toep_cfg2.txt", "dram_bytes_per_slot_mode1"),
+                 "xtoep_mid": ("xtoep_cfg2.txt", "dram_bytes_per_slot"),
+                 "xtoep_fwd": ("xtoep_cfg2.txt", "dram_bytes_per_slot_mode0")}
+
+
 def dram_traffic_from_profile(kind):
     """Per-slot DRAM bytes of a kernel from a committed ncu summary
-    (profiles/<kind>_cfg2.txt, line 'dram_bytes_per_slot: <float>')."""
-    p = os.path.join(ROOT, "profiles", f"{kind}_cfg2.txt")
+    (profiles/<kind>_cfg2.txt, or the file PROFILE_LINES names; a line
+    '<key>: <float>')."""
+    name, key = PROFILE_LINES.get(kind, (f"{kind}_cfg2.txt", "dram_bytes_per_slot"))
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_slot:"):
+        if line.startswith(key + ":"):
             return float(line.split(":", 1)[1])
     return None
 
@@ -505,6 +521,8 @@ def run_ours(args):
                           for op in ops}
     if rank == 0 and world == 1 and args.uneven_scale > 0:
         line["uneven_batch"] = uneven_leg(args, args.uneven_scale)
+    if rank == 0 and world == 1 and args.loo_scale > 0:
+        line["loo_sweep"] = loo_leg(args, args.loo_scale)
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_leg(tilts, rows[0], plan)
         if "value" in line["reference_gpu"]:
@@ -518,11 +536,43 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+WARM_TOLS, WARM_CHECK = (0.03, 0.02), 10   # relative-step tolerances of the warm and cold solves
+
+
+def conv_rates(dev):
+    """CUDA-event TFLOP/s of the network's tensor-core 3x3 convolution
+    (icon_ws_conv3x3: tcgen05.mma fed by TMA, BF16 in, FP32 accumulate) on
+    the shapes of its levels for 32 images of 304 x 1024."""
+    import torch
+    from feilab_b200 import warmstart
+    out = {}
+    for c, H, W in ((16, 304, 1024), (32, 152, 512), (64, 76, 256), (128, 38, 128)):
+        x = torch.randn((32, H, W, c), device=dev).to(torch.bfloat16)
+        w = (0.05 * torch.randn((9, c, c), device=dev)).to(torch.bfloat16)
+        for _ in range(3):
+            warmstart.conv3x3(x, w)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 20
+        e0.record()
+        for _ in range(reps):
+            warmstart.conv3x3(x, w)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        tf = 2.0 * 32 * H * W * c * c * 9 / (ms / 1e3) / 1e12
+        out[f"{c}ch_{H}x{W}"] = {"ms": round(ms, 4), "tflops": round(tf, 1)}
+    return out
+
+
 def warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S):
-    """The learned warm start against the plain solve on the same slices:
-    timed input stage + network + full schedule (device-resident inputs),
-    the FRC of its result against the plain result (the acceptance check), and the
-    held-out iterations-to-tolerance comparison stored with the weights."""
+    """The learned warm start against the plain solve on the same slices,
+    both stopped at each relative-step tolerance of WARM_TOLS: cold = input stage
+    + icon_solve_until from m = 0; warm = input stage + network +
+    icon_solve_warm (the warm solve to the tolerance, the per-slice
+    acceptance test and the cold redo of rejected slices).  Device-resident
+    rows, CUDA events; the FRC of both against the full-schedule cold result,
+    the slices the acceptance test sent back, and the held-out comparison
+    stored with the weights."""
     import torch
     from feilab_b200 import sharding, warmstart
     from feilab_b200.train_warmstart import frc_mean
@@ -534,42 +584,69 @@ def warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S):
     net = warmstart.Network(plan, capacity=cap)
     net.set_params(params, gain)
 
-    def step(i):
-        A = plan.prepare_rhs(rows[i])
-        m0 = torch.empty((S, NX, THICK), dtype=torch.float32, device=A.device)
-        for s0 in range(0, S, cap):
-            net.predict(A[s0:s0 + cap], out=m0[s0:s0 + cap])
-        return A, m0, plan.solve(A, SCHED, DATA_TYPE, THRESHOLD, m0=m0)
+    def run(tol):
+        def cold(i):
+            A = plan.prepare_rhs(rows[i])
+            m, it, _ = plan.solve_until(A, tol, SCHED, DATA_TYPE, THRESHOLD, check_every=WARM_CHECK)
+            return A, m, it, None
 
-    steps = min(args.steps, 5)
-    for i in range(args.warmup):
-        step(i)
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for i in range(args.warmup, args.warmup + steps):
-        A, m0, m_warm = step(i)
-    e1.record(stream)
-    barrier()
-    t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-    # inference alone, and the acceptance check: FRC of the warm result against the cold one
+        def warm(i):
+            A = plan.prepare_rhs(rows[i])
+            m0 = torch.empty((S, NX, THICK), dtype=torch.float32, device=A.device)
+            for s0 in range(0, S, cap):
+                net.predict(A[s0:s0 + cap], out=m0[s0:s0 + cap])
+            m, why, it = plan.solve_warm(A, m0, tol, SCHED, DATA_TYPE, THRESHOLD, check_every=WARM_CHECK)
+            return A, m, it, why
+
+        res = {}
+        for name, fn in (("cold_to_tol", cold), ("warm_to_tol", warm)):
+            for i in range(min(args.warmup, 1)):
+                fn(i)
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            its, redone = [], 0
+            for i in range(args.warmup, args.warmup + steps):
+                A, m, it, why = fn(i)
+                its.append(it)
+                if why is not None:
+                    redone += int((why != 0).sum())
+            e1.record(stream)
+            barrier()
+            t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+            res[name] = {"value": sharding.job_rate(world, S, steps, t), "unit": "slices/s", "iterations": its,
+                         "m_last": m}
+            if why is not None:
+                res[name]["redone_cold"] = redone
+                res[name]["slices"] = S * steps
+        # both against the full-schedule cold result of the last step's slices
+        m_full = plan.solve(A, SCHED, DATA_TYPE, THRESHOLD)
+        torch.cuda.synchronize()
+        for name in res:
+            f = frc_mean(res[name].pop("m_last")[:16].double().cpu(), m_full[:16].double().cpu())
+            res[name]["frc_vs_full_cold_min"] = round(float(f.min()), 4)
+        res["gain"] = round(res["warm_to_tol"]["value"] / res["cold_to_tol"]["value"], 3)
+        return res, A
+
+    steps = min(args.steps, 3)
+    by_tol = {}
+    for tol in WARM_TOLS:
+        by_tol[str(tol)], A = run(tol)
+    # inference alone
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0 = torch.empty((S, NX, THICK), dtype=torch.float32, device=A.device)
     f0.record(stream)
     for s0 in range(0, S, cap):
         net.predict(A[s0:s0 + cap], out=m0[s0:s0 + cap])
     f1.record(stream)
-    m_cold = plan.solve(A, SCHED, DATA_TYPE, THRESHOLD)
     torch.cuda.synchronize()
-    frc = frc_mean(m_warm[:16], m_cold[:16])
     net.close()
-    return {"value": sharding.job_rate(world, S, steps, t), "unit": "slices/s", "steps": steps,
-            "schedule": "network start + the full reference schedule", "inference_ms_per_slice":
-            round(f0.elapsed_time(f1) / S, 4), "frc_vs_cold_min": round(float(frc.min()), 4),
+    return {"check_every": WARM_CHECK, "by_tolerance": by_tol,
+            "inference_ms_per_slice": round(f0.elapsed_time(f1) / S, 4),
+            "conv_tensor_core": {**conv_rates(A.device), **bf16_peak()},
             "heldout_icon_iterations_to_frc_0.99": {"cold": meta.get("icon_iters_to_frc099_cold"),
                                                     "warm": meta.get("icon_iters_to_frc099_warm")},
             "heldout_prediction_frc_min": meta.get("prediction_frc_min"),
-            "gain_to_tolerance": (round(meta["icon_iters_to_frc099_cold"] / meta["icon_iters_to_frc099_warm"], 3)
-                                  if meta.get("icon_iters_to_frc099_warm") else None),
             "weights": f"feilab_b200/weights/warmstart_{NX}x{THICK}.npz (trained on {meta.get('train_slices')} slices)"}
 
 
@@ -635,6 +712,55 @@ def uneven_leg(args, slice_scale):
             "iterations": sum(SCHED), "operator": "toeplitz"}
 
 
+def loo_leg(args, slice_scale):
+    """Leave-one-out cross validation of the 1024-wide, 61-tilt workload
+    (SNR 0.1, thickness 300, the full 10,280,10 schedule) on 512 * slice_scale
+    slices: every tilt left out in turn, 61 x slices solves.  The batched
+    sweep (icon_loo_sweep: one plan over all tilts, one slice group per
+    (omitted tilt, 8 slices) with that tilt's weights at 0, all solves in one
+    batched schedule) against the plain sweep (a plan rebuilt without each
+    tilt, its slices solved and reprojected at the omitted angle, as the
+    reference's Lib_2D_crossV2 does for its one tilt), both cold-started and
+    with the Toeplitz operator; wall time around each, per-tilt FRC of both."""
+    import torch
+    from feilab_b200 import icon, tools
+    S = max(8, int(round(512 * slice_scale)))
+    rows, tilts = make_rows(list(range(S)), "cuda")
+    rows = rows.cpu().numpy()
+    nz = len(tilts)
+    t0 = time.perf_counter()
+    frc_b, _, _ = tools.loo_sweep(rows, THICK, tilts, SCHED, DATA_TYPE, THRESHOLD, capacity=SLICES_PER_STEP,
+                                  operator="toeplitz")
+    t_b = time.perf_counter() - t0
+    cap = min(SLICES_PER_STEP, S)
+    frc_p = np.zeros_like(frc_b)
+    t0 = time.perf_counter()
+    for k in range(nz):
+        keep = [i for i in range(nz) if i != k]
+        p = icon.IconPlan(NX, THICK, tilts[keep], capacity=cap)
+        p.set_operator("toeplitz")
+        rp = np.zeros((S, NX), np.float32)
+        for s0 in range(0, S, cap):
+            n = min(cap, S - s0)
+            r = torch.from_numpy(np.ascontiguousarray(rows[s0:s0 + n][:, keep])).cuda()
+            m = p.solve(p.prepare_rhs(r), SCHED, DATA_TYPE, THRESHOLD)
+            rp[s0:s0 + n] = p.reproject(m, float(tilts[k])).cpu().numpy()
+        p.close()
+        frc_p[k] = tools.frc(rows[:, k, :], rp)
+    t_p = time.perf_counter() - t0
+    mean_b, mean_p = frc_b[:, 1:].mean(axis=1), frc_p[:, 1:].mean(axis=1)
+    return {"workload": f"1024 wide x {S} slices x {nz} tilts (-60..60 step 2), SNR 0.1, thickness {THICK}, "
+                        f"{sum(SCHED)} iterations, every tilt left out in turn", "solves": nz * S,
+            "batched": {"seconds": round(t_b, 2), "solves_per_s": round(nz * S / t_b, 1)},
+            "plain_per_tilt_plans": {"seconds": round(t_p, 2), "solves_per_s": round(nz * S / t_p, 1)},
+            "speedup": round(t_p / t_b, 3),
+            "frc_mean_per_tilt": {"batched_min": round(float(mean_b.min()), 4),
+                                  "batched_max": round(float(mean_b.max()), 4),
+                                  "max_abs_diff_vs_plain": float(np.abs(frc_b - frc_p).max())},
+            "frc_mean_per_tilt_batched": [round(float(v), 4) for v in mean_b],
+            "operator": "toeplitz", "start": "m = 0 (a warm start would leak the held-out projection)"}
+
+
 def run_profile_case(args):
     """Small case for ncu captures: --profile-slices slices of the workload
     (32 by default: the grid intermediate of every kernel, 157 MB, is larger
@@ -671,6 +797,9 @@ def main():
     ap.add_argument("--uneven-scale", type=float, default=0.25,
                     help="slice-count scale of the 24-series uneven batch leg (0 skips it; 1 is the full workload)")
     ap.add_argument("--uneven-only", action="store_true", help="run the uneven batch leg only and print it")
+    ap.add_argument("--loo-scale", type=float, default=1.0 / 16,
+                    help="slice-count scale of the leave-one-out leg (512 slices x scale; 0 skips it)")
+    ap.add_argument("--loo-only", action="store_true", help="run the leave-one-out leg only and print it")
     ap.add_argument("--tune-write", default=None,
                     help="tuning cache file to read and extend (time every shape missing from it)")
     ap.add_argument("--profile", action="store_true", help="run the small ncu case only")
@@ -683,6 +812,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         print(json.dumps({"uneven_batch": uneven_leg(args, args.uneven_scale)}), flush=True)
+        return
+    if args.loo_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"loo_sweep": loo_leg(args, args.loo_scale)}), flush=True)
         return
     if args.warmup < 3:
         args.warmup = 3

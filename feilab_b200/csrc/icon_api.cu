@@ -228,6 +228,10 @@ struct icon_plan {
     float *cx = nullptr, *cy = nullptr, *rcx = nullptr, *rcy = nullptr, *phi1 = nullptr;
     int *i10 = nullptr;
     float2 *tw0 = nullptr, *tw0h = nullptr, *tw1 = nullptr;
+    // Length of the Toeplitz y-transforms: the smallest 32 R >= 2 N1 - 1 that
+    // k_ytoep4 takes (at most n1), else n1; tw1t its twiddles.
+    int n1t = 0;
+    float2 *tw1t = nullptr;
     // scratch sized for Gcap groups
     float2 *G1 = nullptr, *P = nullptr, *f = nullptr, *rhat = nullptr, *Ahwb = nullptr, *imgc = nullptr;
     float *m = nullptr, *rows = nullptr, *outrp = nullptr, *mout = nullptr;
@@ -236,6 +240,11 @@ struct icon_plan {
     double *step_part = nullptr, *step = nullptr;   // relative update size (icon_solve_until)
     float *wgroup = nullptr;   // [Gcap][M] per-group weights while wgroups > 0
     int wgroups = 0;
+    // Distinct weight sets among the groups (Toeplitz kernels are computed
+    // once per set): wuniq [kt_unique][M], kidx [Gcap] the set of each group.
+    float *wuniq = nullptr;
+    int *kidx = nullptr;
+    int kt_unique = 0;
     // Normal operator of the iterations: ICON_OPERATOR_NUFFT (the reference's
     // NUFFT pair) or ICON_OPERATOR_TOEPLITZ (A^H W A as a convolution with Kt).
     int op = ICON_OPERATOR_NUFFT;
@@ -244,7 +253,7 @@ struct icon_plan {
     double stop_tol = 0.0;
     int stop_every = 10;
     float *Kt = nullptr;        // [Gcap][n0][n1] Toeplitz kernels (one used unless per-group weights)
-    int kt_groups = 0;          // kernels computed for: 1 = the plan's weights, Gcap = per-group weights
+    int kt_groups = 0;          // kernels computed: 1, or one per distinct weight set of the groups
     int kt_cap = 0;             // kernels the Kt table has room for
     bool kt_stale = true;
     float *ones0 = nullptr, *ones1 = nullptr;   // unit deapodisation of the Toeplitz x-passes
@@ -309,7 +318,8 @@ struct icon_plan {
         g.ent_lb = t.ent_lb; g.ent_phiy = t.ent_phiy; g.ent_pxy = t.ent_pxy;
         g.tw0 = tw0; g.tw0h = tw0h; g.tw1 = tw1;
         g.Kt = Kt;
-        g.kstride = kt_groups > 1 ? (size_t)n0 * n1 : 0;
+        g.kstride = kt_groups > 1 ? (size_t)n0 * n1t : 0;
+        g.kidx = kt_groups > 1 ? kidx : nullptr;
         return g;
     }
     // The Toeplitz iteration's view: the plan's nodes with unit deapodisation
@@ -319,6 +329,8 @@ struct icon_plan {
         Geo g = geo(nodes);
         g.rcx = ones0;
         g.rcy = ones1;
+        g.n1 = n1t;          // the y-transforms of the convolution
+        g.tw1 = tw1t;
         return g;
     }
     Geo1 geo1() const
@@ -599,23 +611,23 @@ icon_status launch_iteration(icon_plan *p, int G, bool clamp, int data_type, flo
 icon_status ensure_toeplitz(icon_plan *p, cudaStream_t st)
 {
     if (p->op != ICON_OPERATOR_TOEPLITZ || !p->kt_stale) return ICON_OK;
-    const int groups_needed = p->wgroups > 0 ? p->Gcap : 1;
+    const int groups_needed = p->wgroups > 0 ? p->kt_unique : 1;
     if (p->Kt && p->kt_cap < groups_needed) {   // one kernel per group needs a larger table
         p->arena.release(p->Kt);
         p->Kt = nullptr;
     }
     if (!p->Kt) {
-        ICON_TRY(p->arena.alloc(&p->Kt, (size_t)groups_needed * p->n0 * p->n1));
+        ICON_TRY(p->arena.alloc(&p->Kt, (size_t)groups_needed * p->n0 * p->n1t));
         p->kt_cap = groups_needed;
     }
     float *xy_d = nullptr;
     if (!p->nodes_xy) ICON_TRY(p->arena.upload(&p->nodes_xy, p->xy.data(), p->xy.size()));
     xy_d = p->nodes_xy;
-    const float *w = p->wgroups > 0 ? p->wgroup : p->nodes.w;
-    dim3 grid((p->n1 + icon::kToepTile - 1) / icon::kToepTile, (p->n0 + icon::kToepTile - 1) / icon::kToepTile,
+    const float *w = p->wgroups > 0 ? p->wuniq : p->nodes.w;
+    dim3 grid((p->n1t + icon::kToepTile - 1) / icon::kToepTile, (p->n0 + icon::kToepTile - 1) / icon::kToepTile,
               groups_needed);
     icon::k_toep_kernel<<<grid, 256, 0, st>>>(xy_d, w, p->wgroups > 0 ? (size_t)p->M : 0, p->M, p->N0, p->N1, p->n0,
-                                              p->n1, icon::ytoep4_fits(p->n1) ? p->lg1 - 5 : 0, p->Kt);
+                                              p->n1t, icon::ytoep4_fits(p->n1t) ? p->n1t / 32 : 0, p->Kt);
     ICON_CUDA(cudaGetLastError());
     p->kt_groups = groups_needed;
     p->kt_stale = false;
@@ -652,7 +664,7 @@ icon_status launch_iteration_xt_raw(icon_plan *p, int G, bool upd, bool clamp_pr
 {
     Geo g = p->geo_unit();
     const double slots = (double)G * p->B;
-    const double NN = (double)p->N0 * p->N1, G1b = (double)p->n0 * p->N1 * 8, Kb = (double)p->n0 * p->n1 * 4;
+    const double NN = (double)p->N0 * p->N1, G1b = (double)p->n0 * p->N1 * 8, Kb = (double)p->n0 * p->n1t * 4;
     icon::XtArgs xa{};
     xa.N0 = p->N0; xa.N1 = p->N1; xa.n0 = p->n0; xa.tw0 = p->tw0; xa.G1 = p->G1; xa.m = p->m;
     xa.rhat_in = p->rhat; xa.alpha = p->alpha; xa.upd = upd ? 1 : 0; xa.clamp = clamp_prev ? 1 : 0;
@@ -694,7 +706,7 @@ icon_status launch_iteration_toep(icon_plan *p, int G, bool clamp, int data_type
     ICON_TRY(flush_update(p, st));
     Geo g = p->geo_unit();
     const double slots = (double)G * p->B;
-    const double NN = (double)p->N0 * p->N1, G1b = (double)p->n0 * p->N1 * 8, Kb = (double)p->n0 * p->n1 * 4;
+    const double NN = (double)p->N0 * p->N1, G1b = (double)p->n0 * p->N1 * 8, Kb = (double)p->n0 * p->n1t * 4;
     dim3 gx(p->N1, G), gy(G, p->n0);
     WITH_B(p->B,
         LAUNCH_B(p, K_XF, st, (NN * 4 + G1b) * slots, L::xpass_fwd_full(p->ex, gx, p->thr_x, p->smem_x, st, g, p->m, p->G1));
@@ -953,6 +965,24 @@ static icon_status plan_create_impl(const icon_geometry *geo, int group, icon_pl
     p->smem_x = (size_t)p->n0 * B * sizeof(float2);
     p->smem_y = icon::ypass_fwd_smem(p->n1, B);
     p->smem_ya = icon::ypass_adj_smem(p->n1, B);
+    // Toeplitz y-length: a circular convolution of the N1 rows with a kernel
+    // of support 2 N1 - 1 needs 2 N1 - 1 points; the four-step kernel takes
+    // 32 R for R in {4, 6, 8, 10, 12, 16, 20, 24, 32}.  ICON_TOEP_POW2=1 keeps
+    // the power of two n1 (for comparison).
+    p->n1t = p->n1;
+    if (icon::ytoep4_fits(p->n1) && !std::getenv("ICON_TOEP_POW2")) {
+        for (int R : {4, 6, 8, 10, 12, 16, 20, 24, 32})
+            if (32 * R >= 2 * N1 - 1 && 32 * R <= p->n1) {
+                p->n1t = 32 * R;
+                break;
+            }
+    }
+    if (p->n1t == p->n1) {
+        p->tw1t = p->tw1;
+    } else {
+        std::vector<float2> t1t = twiddles(p->n1t);
+        ICON_TRY(p->arena.upload(&p->tw1t, t1t.data(), t1t.size()));
+    }
     p->smem_yt = icon::ypass_toep_smem(p->n1, B);
     int smem_max = 0;
     ICON_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -1058,6 +1088,22 @@ icon_status icon_plan_set_group_weights(icon_plan *p, const float *h_w, int ngro
     ICON_CUDA(cudaMemcpy(p->wgroup, h_w, sizeof(float) * ngroups * M, cudaMemcpyHostToDevice));
     for (int gi = ngroups; gi < p->Gcap; ++gi)   // the remaining groups keep the plan's own weights
         ICON_CUDA(cudaMemcpy(p->wgroup + gi * M, p->nodes.w, sizeof(float) * M, cudaMemcpyDeviceToDevice));
+    // Distinct weight sets, in order of first use: group gi uses set kmap[gi].
+    std::vector<const float *> sets;
+    std::vector<int> kmap(p->Gcap);
+    for (int gi = 0; gi < p->Gcap; ++gi) {
+        const float *v = gi < ngroups ? h_w + (size_t)gi * M : p->w.data();
+        int k = 0;
+        while (k < (int)sets.size() && std::memcmp(sets[k], v, sizeof(float) * M) != 0) ++k;
+        if (k == (int)sets.size()) sets.push_back(v);
+        kmap[gi] = k;
+    }
+    if (!p->wuniq) ICON_TRY(p->arena.alloc(&p->wuniq, (size_t)p->Gcap * M));
+    if (!p->kidx) ICON_TRY(p->arena.alloc(&p->kidx, (size_t)p->Gcap));
+    for (size_t k = 0; k < sets.size(); ++k)
+        ICON_CUDA(cudaMemcpy(p->wuniq + k * M, sets[k], sizeof(float) * M, cudaMemcpyHostToDevice));
+    ICON_CUDA(cudaMemcpy(p->kidx, kmap.data(), sizeof(int) * p->Gcap, cudaMemcpyHostToDevice));
+    p->kt_unique = (int)sets.size();
     p->wgroups = ngroups;
     p->kt_stale = true;
     return ICON_OK;

@@ -501,7 +501,7 @@ int main(int argc, char **argv)
         std::vector<float> frc((size_t)nz * (half > 0 ? half : 1));
         std::vector<int> iters(nz);
         if (icon_loo_sweep(rows.data(), nx, thickness, nz, tilts.data(), &cfg, slicetotal, A.batch, 0.0, A.gpus[0],
-                           frc.data(), nullptr, iters.data()) != ICON_OK) {
+                           frc.data(), nullptr, iters.data(), A.op) != ICON_OK) {
             printf("running state: fail!\nError message: leave-one-out sweep: %s\n", icon_last_error());
             return 1;
         }

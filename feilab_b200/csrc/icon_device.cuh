@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 namespace icon {
 
 constexpr int kTaps = 14;   // 2m+2 taps per dimension, m = 6 (nufft_gpu_v8.cuh:5, NU:226)
@@ -297,6 +299,144 @@ __device__ __forceinline__ void dft_inplace(float2 (&a)[R], float dir)
     if constexpr (R >= 2) dft_stage<R, 2>(a, dir);
 }
 
+// ----------------------------------------------- mixed-radix (3, 5) DFTs ----
+// Twiddles of DFT lengths that are not powers of two, as compile-time
+// constants: cos and sin of 2 pi m / n by their Taylor series in double after
+// reduction to [-pi, pi] (16 terms leave an error below 1e-18), rounded to
+// float once.
+constexpr double kTwoPiD = 6.283185307179586476925286766559;
+__host__ __device__ constexpr double ct_angle(int m, int n)
+{
+    const double t = kTwoPiD * (double)(((m % n) + n) % n) / (double)n;
+    return t > kTwoPiD / 2 ? t - kTwoPiD : t;
+}
+__host__ __device__ constexpr double ct_sin(double x)
+{
+    double term = x, sum = x;
+    for (int k = 1; k < 16; ++k) {
+        term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+__host__ __device__ constexpr double ct_cos(double x)
+{
+    double term = 1.0, sum = 1.0;
+    for (int k = 1; k < 16; ++k) {
+        term *= -x * x / ((2.0 * k - 1.0) * (2.0 * k));
+        sum += term;
+    }
+    return sum;
+}
+
+// v * exp(dir * 2 pi i m / n), the factor a compile-time constant.
+template <int N, int M>
+__device__ __forceinline__ float2 tw_mul(float2 v, float dir)
+{
+    if constexpr (M % N == 0) {
+        return v;
+    } else {
+        constexpr float c = (float)ct_cos(ct_angle(M, N)), s = (float)ct_sin(ct_angle(M, N));
+        const float sd = dir * s;
+        return make_float2(fmaf(v.x, c, -sd * v.y), fmaf(v.x, sd, v.y * c));
+    }
+}
+
+// 3- and 5-point DFTs in place (natural order), sign dir.  With
+// w = exp(dir 2 pi i / P): X_k = sum_r x_r w^(r k), written as sums and
+// differences of the symmetric pairs x_r +- x_(P-r).
+__device__ __forceinline__ void dft3(float2 (&a)[3], float dir)
+{
+    constexpr float h = 0.8660254037844386f;   // sin(2 pi / 3)
+    const float2 s = add2(a[1], a[2]), d = sub2(a[1], a[2]);
+    const float2 m = make_float2(fmaf(-0.5f, s.x, a[0].x), fmaf(-0.5f, s.y, a[0].y));
+    const float hd = dir * h;
+    const float2 id = make_float2(-hd * d.y, hd * d.x);   // i dir h (x1 - x2)
+    a[0] = add2(a[0], s);
+    a[1] = add2(m, id);
+    a[2] = sub2(m, id);
+}
+
+__device__ __forceinline__ void dft5(float2 (&a)[5], float dir)
+{
+    constexpr float c1 = (float)ct_cos(ct_angle(1, 5)), c2 = (float)ct_cos(ct_angle(2, 5));
+    constexpr float s1 = (float)ct_sin(ct_angle(1, 5)), s2 = (float)ct_sin(ct_angle(2, 5));
+    const float2 t1 = add2(a[1], a[4]), t2 = add2(a[2], a[3]), t3 = sub2(a[1], a[4]), t4 = sub2(a[2], a[3]);
+    const float2 x0 = a[0];
+    const float2 p1 = make_float2(fmaf(c2, t2.x, fmaf(c1, t1.x, x0.x)), fmaf(c2, t2.y, fmaf(c1, t1.y, x0.y)));
+    const float2 p2 = make_float2(fmaf(c1, t2.x, fmaf(c2, t1.x, x0.x)), fmaf(c1, t2.y, fmaf(c2, t1.y, x0.y)));
+    // q1 = dir (s1 t3 + s2 t4), q2 = dir (s2 t3 - s1 t4); X1,4 = p1 +- i q1, X2,3 = p2 +- i q2
+    const float2 q1 = make_float2(dir * fmaf(s1, t3.x, s2 * t4.x), dir * fmaf(s1, t3.y, s2 * t4.y));
+    const float2 q2 = make_float2(dir * fmaf(s2, t3.x, -s1 * t4.x), dir * fmaf(s2, t3.y, -s1 * t4.y));
+    a[0] = add2(x0, add2(t1, t2));
+    a[1] = make_float2(p1.x - q1.y, p1.y + q1.x);
+    a[4] = make_float2(p1.x + q1.y, p1.y - q1.x);
+    a[2] = make_float2(p2.x - q2.y, p2.y + q2.x);
+    a[3] = make_float2(p2.x + q2.y, p2.y - q2.x);
+}
+
+template <int P>
+__device__ __forceinline__ void dft_small(float2 (&a)[P], float dir)
+{
+    static_assert(P == 3 || P == 5, "radix 3 or 5");
+    if constexpr (P == 3) dft3(a, dir);
+    else dft5(a, dir);
+}
+
+// Twiddles y[q][k1] *= exp(dir 2 pi i q k1 / R) of the mixed-radix step,
+// each factor a compile-time constant (index sequences unroll q and k1).
+template <int R, int P, int Q, int q, int... K1>
+__device__ __forceinline__ void tw_row(float2 (&yq)[P], float dir, std::integer_sequence<int, K1...>)
+{
+    ((yq[K1] = tw_mul<R, q * K1>(yq[K1], dir)), ...);
+}
+template <int R, int P, int Q, int... Qs>
+__device__ __forceinline__ void tw_all(float2 (&y)[Q][P], float dir, std::integer_sequence<int, Qs...>)
+{
+    (tw_row<R, P, Q, Qs>(y[Qs], dir, std::make_integer_sequence<int, P>{}), ...);
+}
+
+// DFT of R values in registers, natural order in and out:
+// a[k] <- sum_r a[r] exp(dir 2 pi i r k / R).  R a power of two (radix-2
+// DIT above, after a bit-reversal that only renames registers) or R = P Q with
+// P = 3 or 5 and Q a power of two (Cooley-Tukey: P-point DFTs over
+// r = Q p + q, twiddles exp(dir 2 pi i q k1 / R), Q-point DFTs over q, k =
+// k1 + P k2).
+template <int R>
+__device__ __forceinline__ void dft_nat(float2 (&a)[R], float dir)
+{
+    if constexpr ((R & (R - 1)) == 0) {
+        constexpr int L = Lg<R>::v;
+        float2 t[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) t[brev5(r) >> (5 - L)] = a[r];
+        dft_inplace<R>(t, dir);
+#pragma unroll
+        for (int r = 0; r < R; ++r) a[r] = t[r];
+    } else {
+        constexpr int P = (R % 5 == 0) ? 5 : 3, Q = R / P;
+        static_assert(R % P == 0 && (Q & (Q - 1)) == 0 && Q <= 32, "R = 3 or 5 times a power of two");
+        constexpr int LQ = Lg<Q>::v;
+        float2 y[Q][P];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) y[q][p] = a[Q * p + q];
+            dft_small<P>(y[q], dir);
+        }
+        tw_all<R, P, Q>(y, dir, std::make_integer_sequence<int, Q>{});
+#pragma unroll
+        for (int k1 = 0; k1 < P; ++k1) {
+            float2 u[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) u[LQ ? (brev5(q) >> (5 - LQ)) : 0] = y[q][k1];
+            dft_inplace<Q>(u, dir);
+#pragma unroll
+            for (int k2 = 0; k2 < Q; ++k2) a[k1 + P * k2] = u[k2];
+        }
+    }
+}
+
 // One radix-2 decimation-in-frequency stage (butterfly span LEN), then the
 // next, shorter one.
 template <int R, int LEN>
@@ -516,7 +656,15 @@ __device__ __forceinline__ double block_sum_per_slice(double v, double *scratch,
 {
     scratch[threadIdx.x] = v;
     __syncthreads();
-    for (int stride = blockDim.x >> 1; stride >= B; stride >>= 1) {
+    // A block of T threads that is not a power of two (the Toeplitz y-pass
+    // of a mixed-radix length) first folds threads P2.. onto 0.. (P2 the
+    // largest power of two below T, a multiple of B, so slices stay apart).
+    const int P2 = 1 << (31 - __clz((int)blockDim.x));
+    if (P2 < (int)blockDim.x) {
+        if ((int)threadIdx.x < (int)blockDim.x - P2) scratch[threadIdx.x] += scratch[threadIdx.x + P2];
+        __syncthreads();
+    }
+    for (int stride = P2 >> 1; stride >= B; stride >>= 1) {
         if ((int)threadIdx.x < stride) scratch[threadIdx.x] += scratch[threadIdx.x + stride];
         __syncthreads();
     }

@@ -41,18 +41,24 @@ void Launch<B>::xpass_fwd_full(int E, dim3 grid, int threads, size_t smem, cudaS
     else k_xpass_fwd<true, B, 16, true><<<grid, threads, smem, st>>>(g, in, G1);
 }
 
-// The four-step register FFT (k_ytoep4) for n1 = 128 .. 1024; blockDim =
-// n1*B/32, shared memory n1*B float2.
+// The four-step register FFT (k_ytoep4) for n1 = 32 R, R in
+// {4, 6, 8, 10, 12, 16, 20, 24, 32}; blockDim = n1*B/32, shared memory
+// n1*B float2.
 template <int B, int MODE>
 static void launch_ytoep4(dim3 grid, cudaStream_t st, const Geo &g, float2 *G1, double *part)
 {
     const int threads = g.n1 * B / 32;
     const size_t smem = ytoep4_smem(g.n1, B);
-    switch (g.lg1) {
-    case 7: k_ytoep4<B, 2, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
-    case 8: k_ytoep4<B, 3, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
-    case 9: k_ytoep4<B, 4, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
-    default: k_ytoep4<B, 5, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    switch (g.n1 / 32) {
+    case 4: k_ytoep4<B, 4, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    case 6: k_ytoep4<B, 6, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    case 8: k_ytoep4<B, 8, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    case 10: k_ytoep4<B, 10, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    case 12: k_ytoep4<B, 12, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    case 16: k_ytoep4<B, 16, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    case 20: k_ytoep4<B, 20, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    case 24: k_ytoep4<B, 24, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
+    default: k_ytoep4<B, 32, MODE><<<grid, threads, smem, st>>>(g, G1, part); break;
     }
 }
 
@@ -257,14 +263,24 @@ cudaError_t Launch<B>::set_smem(int ex, int ey, size_t, size_t, size_t, size_t, 
     set((const void *)k_ypass_adj<B, 16, true>);
     set((const void *)k_ypass_toep<B, 16>);
     set((const void *)k_ypass_toep_quad<B, 16>);
-    set((const void *)k_ytoep4<B, 2, 0>);
-    set((const void *)k_ytoep4<B, 3, 0>);
     set((const void *)k_ytoep4<B, 4, 0>);
-    set((const void *)k_ytoep4<B, 5, 0>);
-    set((const void *)k_ytoep4<B, 2, 1>);
-    set((const void *)k_ytoep4<B, 3, 1>);
+    set((const void *)k_ytoep4<B, 6, 0>);
+    set((const void *)k_ytoep4<B, 8, 0>);
+    set((const void *)k_ytoep4<B, 10, 0>);
+    set((const void *)k_ytoep4<B, 12, 0>);
+    set((const void *)k_ytoep4<B, 16, 0>);
+    set((const void *)k_ytoep4<B, 20, 0>);
+    set((const void *)k_ytoep4<B, 24, 0>);
+    set((const void *)k_ytoep4<B, 32, 0>);
     set((const void *)k_ytoep4<B, 4, 1>);
-    set((const void *)k_ytoep4<B, 5, 1>);
+    set((const void *)k_ytoep4<B, 6, 1>);
+    set((const void *)k_ytoep4<B, 8, 1>);
+    set((const void *)k_ytoep4<B, 10, 1>);
+    set((const void *)k_ytoep4<B, 12, 1>);
+    set((const void *)k_ytoep4<B, 16, 1>);
+    set((const void *)k_ytoep4<B, 20, 1>);
+    set((const void *)k_ytoep4<B, 24, 1>);
+    set((const void *)k_ytoep4<B, 32, 1>);
     return e;
 }
 

@@ -60,8 +60,10 @@ struct Geo {
     const float2 *tw0;     // [n0] exp(-2 pi i q / n0)
     const float2 *tw0h;    // [n0/2] exp(-2 pi i q / (n0/2))
     const float2 *tw1;     // [n1] exp(-2 pi i q / n1)
-    const float *Kt;       // [n0][n1] Toeplitz kernel of A^H W A, group g's at Kt + g*kstride
-    size_t kstride;        // 0: one kernel for every group; n0*n1: one per group
+    const float *Kt;       // [n0][n1] Toeplitz kernel of A^H W A, group g's at Kt + kidx[g]*kstride
+    size_t kstride;        // 0: one kernel for every group; n0*n1: one per distinct weight set
+    const int *kidx;       // [G] kernel of each group (per-group weights), or null
+
 };
 
 // 1-D row-transform tables (cunfft_initPlan_1d, NU:1298-1391).
@@ -122,6 +124,12 @@ __global__ void k_entry_tables(const int *__restrict__ jt, int E, const float *_
 }
 
 #endif  // ICON_KERNELS_TEMPLATES_ONLY
+
+// Which Toeplitz kernel slice group grp uses: groups with equal weights share one.
+__device__ __forceinline__ size_t toep_kernel_index(const Geo &g, int grp)
+{
+    return g.kidx ? (size_t)__ldg(&g.kidx[grp]) : (size_t)grp;
+}
 
 // Loads B consecutive float2 (16-byte vector loads when B is even).
 template <int B>
@@ -1104,12 +1112,12 @@ __device__ __forceinline__ double dirichlet(double x, double kn, double sa, doub
 
 #ifndef ICON_KERNELS_TEMPLATES_ONLY
 // xy: [M][2] node coordinates, w: [M] weights (group g's at w + g*wstride for
-// blockIdx.z = g); K: [G][n0][n1] float.  With perm_lr > 0 each row is stored
+// blockIdx.z = g); K: [G][n0][n1] float.  With perm_r > 0 each row is stored
 // in the order k_ytoep4 reads it: frequency k1 of row k0 at
-// (k1 mod R) * 32 + k1 / R, R = 2^perm_lr = n1 / 32.
+// (k1 mod R) * 32 + k1 / R, R = perm_r = n1 / 32.
 __global__ void __launch_bounds__(256) k_toep_kernel(const float *__restrict__ xy, const float *__restrict__ w,
                                                      size_t wstride, int M, int N0, int N1, int n0, int n1,
-                                                     int perm_lr, float *__restrict__ K)
+                                                     int perm_r, float *__restrict__ K)
 {
     __shared__ __align__(16) double F0[kToepNodes][kToepTile];   // w_j D_N0(x_j0 - k0/n0)
     __shared__ __align__(16) double F1[kToepNodes][kToepTile];   // D_N1(x_j1 - k1/n1)
@@ -1181,7 +1189,7 @@ __global__ void __launch_bounds__(256) k_toep_kernel(const float *__restrict__ x
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
             const int k1 = k1b + 4 * tx + jj;
-            const int pos = perm_lr > 0 ? ((k1 & ((1 << perm_lr) - 1)) << 5) + (k1 >> perm_lr) : k1;
+            const int pos = perm_r > 0 ? (k1 % perm_r) * 32 + k1 / perm_r : k1;
             if (k0 < n0 && k1 < n1) Kg[(size_t)k0 * n1 + pos] = (float)(acc[i][jj] * scale);
         }
     }
@@ -1215,7 +1223,7 @@ __global__ void FFT_BOUNDS(E) k_ypass_toep(Geo g, float2 *__restrict__ G1)
     const float2 *tws = ypass_tw_shared(n) ? tw_s : g.tw1;
     float2 *row = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
     copy_async(buf, row, (size_t)N1 * B * sizeof(float2));        // [N1][B], contiguous
-    copy_async(krow, g.Kt + grp * g.kstride + (size_t)x * n, (size_t)n * sizeof(float));
+    copy_async(krow, g.Kt + toep_kernel_index(g, grp) * g.kstride + (size_t)x * n, (size_t)n * sizeof(float));
     if (ypass_tw_shared(n)) copy_async(tw_s, g.tw1, (size_t)n * sizeof(float2));
     cp_async_commit();
     cp_async_wait<0>();
@@ -1252,7 +1260,7 @@ __global__ void FFT_BOUNDS(E) k_ypass_toep_quad(Geo g, const float2 *__restrict_
     const float2 *tws = ypass_tw_shared(n) ? tw_s : g.tw1;
     const float2 *row = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
     copy_async(buf, row, (size_t)N1 * B * sizeof(float2));
-    copy_async(krow, g.Kt + grp * g.kstride + (size_t)x * n, (size_t)n * sizeof(float));
+    copy_async(krow, g.Kt + toep_kernel_index(g, grp) * g.kstride + (size_t)x * n, (size_t)n * sizeof(float));
     if (ypass_tw_shared(n)) copy_async(tw_s, g.tw1, (size_t)n * sizeof(float2));
     cp_async_commit();
     cp_async_wait<0>();
@@ -1275,49 +1283,63 @@ __global__ void FFT_BOUNDS(E) k_ypass_toep_quad(Geo g, const float2 *__restrict_
 }
 
 // ------------------------------------------- Toeplitz y-passes, 4-step ----
-// The y-direction transforms of the Toeplitz passes for n1 = 32 R
-// (R = 2^LR, 2 <= R <= 32) as a four-step FFT held in registers.  With
+// The y-direction transforms of the Toeplitz passes for a padded length
+// n1 = 32 R (R a power of two from 4 to 32, or 3 or 5 times one: 6, 10, 12,
+// 20, 24) as a four-step FFT held in registers.  The convolution of the
+// thickness-N1 rows with a kernel of support 2 N1 - 1 needs a circular length
+// of at least 2 N1 - 1 and nothing more, so the plan takes the smallest such
+// 32 R (640 for N1 = 300, where the NUFFT grid's power of two is 1024).  With
 // y = 32 a + c (a < R, c < 32) and k = k1 + R k2 (k1 < R, k2 < 32):
 //   X[k1 + R k2] = sum_c w32^(c k2) [ wn^(c k1) sum_a x[32 a + c] wR^(a k1) ],
 // w_L = exp(-2 pi i / L).  A thread of slice b owns 32 values: first the
-// 32/R R-point DFTs over a of its columns c = u + R i, then, after one
-// transpose through shared memory, the 32-point DFT over c of its k1 = u.
-// It then holds X[k1 + R k2] for every k2: a strided set of frequencies,
-// which is all that the pointwise product with K and the quadratic form
-// need.  The inverse runs the same steps backwards from there (32-point
-// inverse DFT, conjugate twiddles, one transpose, R-point inverse DFTs), so
-// the forward-multiply-inverse round trip takes two transposes and no
-// reordering pass.  The N1 inputs of a row are loaded from global memory
+// R-point DFTs over a of its columns c = u, u + R, ... (< 32), then, after
+// one transpose through shared memory, the 32-point DFT over c of its
+// k1 = u.  It then holds X[k1 + R k2] for every k2: a strided set of
+// frequencies, which is all that the pointwise product with K and the
+// quadratic form need.  The inverse runs the same steps backwards from there
+// (32-point inverse DFT, conjugate twiddles, one transpose, R-point inverse
+// DFTs), so the forward-multiply-inverse round trip takes two transposes and
+// no reordering pass.  The N1 inputs of a row are loaded from global memory
 // straight into registers (the B slices of a point are B consecutive float2,
 // so a warp reads 256 contiguous bytes) and the N1 outputs stored from
 // registers; the zero padding is never loaded.  Shared memory holds only the
 // transposed [32][R][B] values, with k1 XOR-swizzled by the low bits of c so
-// that both the column-wise writes and the row-wise reads of a warp are
-// conflict-free (two wavefronts per 32 x 8 bytes).  Each slice's values stay
-// its own, so a slice's result does not depend on its group mates.
-template <int B, int LR>
+// that the column-wise writes and row-wise reads of a warp spread over the
+// banks (for a power-of-two R two wavefronts per 32 x 8 bytes).  Each
+// slice's values stay its own, so a slice's result does not depend on its
+// group mates.
+template <int B, int R>
 __device__ __forceinline__ int ytoep4_sidx(int c, int k1, int b)
 {
-    constexpr int R = 1 << LR;
-    constexpr int SWM = (R - 1) & (16 / B - 1);
-    return ((c * R + (k1 ^ (c & SWM))) << Log2B<B>::v) + b;
+    constexpr int LB = Log2B<B>::v;
+    // XOR mask: below 16/B (a quarter warp's columns) and within the largest
+    // power of two dividing R, so that k1 ^ mask stays below R.
+    constexpr int LOW = R & -R, CAP = 16 / B;
+    constexpr int SWM = (LOW < CAP ? LOW : CAP) - 1;
+    return ((c * R + (k1 ^ (c & SWM))) << LB) + b;
+}
+
+// Lengths R of the first step k_ytoep4 is built for.
+__host__ __device__ constexpr bool ytoep4_radix_ok(int R)
+{
+    return R == 4 || R == 6 || R == 8 || R == 10 || R == 12 || R == 16 || R == 20 || R == 24 || R == 32;
 }
 
 // MODE 0: row x of G1 <- crop F^-1(K[x][.] . F(pad row)), in place (the
 // Toeplitz y-pass of A^H W A m).  MODE 1: part[G][n0][B] <- per slice
 // sum_k K[x][k] |F(pad row)[k]|^2 in FP64 (the step length's denominator).
-template <int B, int LR, int MODE>
-__global__ void __launch_bounds__((1 << LR) * B, 512 / ((1 << LR) * B) < 32 ? 512 / ((1 << LR) * B) : 32)
+// g.n1 = 32 R and g.tw1 its twiddles (the Toeplitz view of the plan).
+template <int B, int R, int MODE>
+__global__ void __launch_bounds__(R * B, 512 / (R * B) < 32 ? 512 / (R * B) : 32)
     k_ytoep4(Geo g, float2 *__restrict__ G1, double *__restrict__ part)
 {
-    constexpr int R = 1 << LR;
     constexpr int LB = Log2B<B>::v;
-    constexpr int NI = 32 / R;
+    constexpr int NI = (32 + R - 1) / R;     // columns per thread in the first step (the last may be short)
     extern __shared__ float2 s[];
     const int grp = blockIdx.x, x = blockIdx.y, N1 = g.N1;
     const int t = threadIdx.x, b = t & (B - 1), u = t >> LB;
     float2 *row = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
-    const float *krow = g.Kt + grp * g.kstride + (size_t)x * (32 * R);
+    const float *krow = g.Kt + toep_kernel_index(g, grp) * g.kstride + (size_t)x * (32 * R);
 
     // Step 1: R-point DFTs over a, twiddles wn^(c k1), transpose.
     {
@@ -1325,16 +1347,17 @@ __global__ void __launch_bounds__((1 << LR) * B, 512 / ((1 << LR) * B) < 32 ? 51
 #pragma unroll
         for (int i = 0; i < NI; ++i) {
             const int c = u + R * i;
+            if (c >= 32) break;
             const float2 *rb = row + (c * B + b);   // point y = 32 a + c at rb[32 B a]
             const int na = (N1 - c + 31) >> 5;      // points y < N1
 #pragma unroll
-            for (int a = 0; a < R; ++a)
-                v[i][brev5(a) >> (5 - LR)] = a < na ? rb[32 * B * a] : make_float2(0.f, 0.f);
+            for (int a = 0; a < R; ++a) v[i][a] = a < na ? rb[32 * B * a] : make_float2(0.f, 0.f);
         }
 #pragma unroll
         for (int i = 0; i < NI; ++i) {
             const int c = u + R * i;
-            dft_inplace<R>(v[i], -1.f);
+            if (c >= 32) break;
+            dft_nat<R>(v[i], -1.f);
             // wn^(c k1): from the table at k1 = 0, 8, 16, 24, stepped by
             // wn^c in between (at most 7 products from a table value).
             const float2 w1 = __ldg(&g.tw1[c]);
@@ -1346,14 +1369,14 @@ __global__ void __launch_bounds__((1 << LR) * B, 512 / ((1 << LR) * B) < 32 ? 51
                 v[i][k1] = cmul(v[i][k1], tw);
             }
 #pragma unroll
-            for (int k1 = 0; k1 < R; ++k1) s[ytoep4_sidx<B, LR>(c, k1, b)] = v[i][k1];
+            for (int k1 = 0; k1 < R; ++k1) s[ytoep4_sidx<B, R>(c, k1, b)] = v[i][k1];
         }
     }
     __syncthreads();
     // Step 2: 32-point DFT over c for k1 = u: w[k2] = X[u + R k2].
     float2 w[32];
 #pragma unroll
-    for (int c = 0; c < 32; ++c) w[brev5(c)] = s[ytoep4_sidx<B, LR>(c, u, b)];
+    for (int c = 0; c < 32; ++c) w[brev5(c)] = s[ytoep4_sidx<B, R>(c, u, b)];
     dft_inplace<32>(w, -1.f);
     // K[x][u + R k2] for k2 = 0..31: 32 consecutive floats of the permuted row.
     const float4 *kq = reinterpret_cast<const float4 *>(krow + 32 * u);
@@ -1402,16 +1425,17 @@ __global__ void __launch_bounds__((1 << LR) * B, 512 / ((1 << LR) * B) < 32 ? 51
         }
         __syncthreads();   // every read of s is done before it is overwritten
 #pragma unroll
-        for (int c = 0; c < 32; ++c) s[ytoep4_sidx<B, LR>(c, u, b)] = w[brev5(c)];
+        for (int c = 0; c < 32; ++c) s[ytoep4_sidx<B, R>(c, u, b)] = w[brev5(c)];
         __syncthreads();
         // R-point inverse DFTs over k1 for columns c = u + R i; rows y < N1 out.
 #pragma unroll
         for (int i = 0; i < NI; ++i) {
             const int c = u + R * i;
+            if (c >= 32) break;
             float2 v[R];
 #pragma unroll
-            for (int k1 = 0; k1 < R; ++k1) v[brev5(k1) >> (5 - LR)] = s[ytoep4_sidx<B, LR>(c, k1, b)];
-            dft_inplace<R>(v, +1.f);
+            for (int k1 = 0; k1 < R; ++k1) v[k1] = s[ytoep4_sidx<B, R>(c, k1, b)];
+            dft_nat<R>(v, +1.f);
             float2 *rb = row + (c * B + b);
             const int na = (N1 - c + 31) >> 5;
 #pragma unroll
@@ -1421,10 +1445,9 @@ __global__ void __launch_bounds__((1 << LR) * B, 512 / ((1 << LR) * B) < 32 ? 51
     }
 }
 
-// Shared memory of k_ytoep4: the transposed [32][R][B] values.
 __host__ __device__ inline size_t ytoep4_smem(int n1, int B) { return (size_t)n1 * B * sizeof(float2); }
-// n1 sizes k_ytoep4 takes (R = n1 / 32 from 4 to 32).
-__host__ __device__ inline bool ytoep4_fits(int n1) { return n1 >= 128 && n1 <= 1024; }
+// n1 sizes k_ytoep4 takes (n1 = 32 R, R in ytoep4_radix_ok).
+__host__ __device__ inline bool ytoep4_fits(int n1) { return n1 % 32 == 0 && ytoep4_radix_ok(n1 / 32); }
 
 }  // namespace icon
 

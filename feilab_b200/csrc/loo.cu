@@ -72,7 +72,7 @@ struct CurrentDevice {
 
 extern "C" icon_status icon_loo_sweep(const float *h_rows, int nx, int thickness, int nz, const float *tilt_deg,
                                       const icon_solve_cfg *cfg, int S, int capacity, double tol, int device,
-                                      float *h_frc, float *h_reproj, int *h_iters)
+                                      float *h_frc, float *h_reproj, int *h_iters, int op)
 {
     if (!h_rows || !tilt_deg || !cfg || !h_frc || nx < 2 || thickness < 1 || nz < 3 || S < 1 || capacity < 1)
         return loo_fail(ICON_ERR_INVALID, "icon_loo_sweep: bad argument");
@@ -84,6 +84,7 @@ extern "C" icon_status icon_loo_sweep(const float *h_rows, int nx, int thickness
     icon_geometry g{nx, thickness, nz, tilt_deg, cap, device};
     Plan P;
     if ((rc = icon_plan_create(&g, &P.p)) != ICON_OK) return rc;
+    if ((rc = icon_plan_set_operator(P.p, op)) != ICON_OK) return rc;
     int dims[10];
     if ((rc = icon_plan_query(P.p, dims)) != ICON_OK) return rc;
     const int M = dims[4], B = dims[6];

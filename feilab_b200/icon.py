@@ -277,7 +277,7 @@ class IconPlan:
                                       step.ctypes.data_as(ctypes.c_void_p), _stream()))
         return m, int(n.value), step
 
-    def solve_warm(self, Ahwb, m0, tol, iters=(0, 10, 0), data_type=1, threshold=0.03, check_every=10, max_dist=1.0):
+    def solve_warm(self, Ahwb, m0, tol, iters=(0, 10, 0), data_type=1, threshold=0.03, check_every=10, max_dist=2.0):
         """Warm-started solve from m0 with the cold start as judge and
         fallback (icon_solve_warm): returns (m, per-slice outcome codes
         ICON_WARM_* as an int array, 0 = accepted, else redone from m = 0,

@@ -133,15 +133,16 @@ def frc(a, b, smooth_overlap=10):
 
 
 def loo_sweep(rows, thickness, tilts, iters=(0, 10, 0), data_type=1, threshold=0.03, capacity=64, tol=0.0,
-              device=0):
+              device=0, operator="nufft"):
     """Leave-one-out cross validation over every tilt: rows (S, nz, nx)
-    float32 (host).  Returns (frc (nz, nx/2), reprojections (nz, S, nx),
+    float32 (host); operator "nufft" or "toeplitz" (the iterations' normal
+    operator).  Returns (frc (nz, nx/2), reprojections (nz, S, nx),
     iterations per omitted tilt (nz,))."""
     from .icon import SolveCfg
     L = lib()
     if not getattr(L, "_loo_ready", False):
         V, I = ctypes.c_void_p, ctypes.c_int
-        L.icon_loo_sweep.argtypes = [V, I, I, I, V, ctypes.POINTER(SolveCfg), I, I, ctypes.c_double, I, V, V, V]
+        L.icon_loo_sweep.argtypes = [V, I, I, I, V, ctypes.POINTER(SolveCfg), I, I, ctypes.c_double, I, V, V, V, I]
         L.icon_loo_sweep.restype = ctypes.c_int
         L._loo_ready = True
     r = np.ascontiguousarray(np.asarray(rows, np.float32))
@@ -155,5 +156,5 @@ def loo_sweep(rows, thickness, tilts, iters=(0, 10, 0), data_type=1, threshold=0
     _check(L.icon_loo_sweep(r.ctypes.data_as(ctypes.c_void_p), nx, int(thickness), nz, t.ctypes.data_as(ctypes.c_void_p),
                             ctypes.byref(cfg), S, int(capacity), float(tol), int(device),
                             f.ctypes.data_as(ctypes.c_void_p), rp.ctypes.data_as(ctypes.c_void_p),
-                            it.ctypes.data_as(ctypes.c_void_p)))
+                            it.ctypes.data_as(ctypes.c_void_p), {"nufft": 0, "toeplitz": 1}[operator]))
     return f, rp, it

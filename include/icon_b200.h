@@ -263,7 +263,9 @@ typedef struct {
     double tol;          /* relative-step tolerance of the ICON phase (> 0), as icon_solve_until */
     int check_every;     /* ICON iterations between checks (>= 1)                               */
     double max_dist;     /* largest accepted ||m - m_infr|| / ||m_infr|| (> 0), m_infr the cold
-                            start's iterate after the first INFR phase                           */
+                            start's iterate after the first INFR phase; the cold result itself
+                            lies 1.0-1.3 from it on synthetic series (the clamped ICON phase adds
+                            the missing-wedge content), so 2 is a working bound                  */
 } icon_warm_cfg;
 
 /* Reasons icon_solve_warm redid a slice from m = 0 (h_redone[s]). */

@@ -96,10 +96,13 @@ icon_status icon_frc(const float *a, const float *b, int nx, int ny, int smooth_
  * h_frc [nz][nx/2] receives the
  * smoothed FRC of each omitted tilt; h_reproj [nz][S][nx] (optional) the
  * reprojections; h_iters[nz] (optional) the iterations of each tilt's
- * longest batch.  Synchronous. */
+ * longest batch.  op is the iterations' normal operator
+ * (ICON_OPERATOR_NUFFT or ICON_OPERATOR_TOEPLITZ, icon_plan_set_operator);
+ * with the Toeplitz operator the groups of a batch that leave out the same
+ * tilt share one kernel.  Synchronous. */
 icon_status icon_loo_sweep(const float *h_rows, int nx, int thickness, int nz, const float *tilt_deg,
                            const icon_solve_cfg *cfg, int S, int capacity, double tol, int device, float *h_frc,
-                           float *h_reproj, int *h_iters);
+                           float *h_reproj, int *h_iters, int op);
 
 #ifdef __cplusplus
 }

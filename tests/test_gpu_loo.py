@@ -61,7 +61,7 @@ def test_loo_with_tolerance_stops_within_schedule(golden):
     assert np.all(np.isfinite(frc_t))
 
 
-def _reduced_plan_reprojection(z, omit):
+def _reduced_plan_reprojection(z, omit, operator="nufft"):
     """The left-out solve of one tilt with a plan built for the series
     without it (the reference's own construction)."""
     import torch
@@ -69,6 +69,7 @@ def _reduced_plan_reprojection(z, omit):
     keep = [k for k in range(len(z["tilts"])) if k != omit]
     S = int(z["S"])
     p = IconPlan(int(z["nx"]), int(z["thickness"]), z["tilts"][keep], capacity=S)
+    p.set_operator(operator)
     rows = torch.from_numpy(np.ascontiguousarray(z["rows"][:, keep])).cuda()
     m = p.solve(p.prepare_rhs(rows), tuple(int(v) for v in z["sched"]), int(z["data_type"]), float(z["threshold"]))
     return p.reproject(m, float(z["tilts"][omit])).cpu().numpy()
@@ -114,3 +115,50 @@ def test_group_weights_set_and_restore(golden):
     p.set_group_weights(None)
     back = p.solve(p.prepare_rhs(rows), sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
     assert np.array_equal(back, plain)
+
+
+@pytest.mark.parametrize("capacity", [4, 24])
+def test_toeplitz_sweep_equals_per_tilt_plans(golden, capacity):
+    # The sweep with the Toeplitz operator: groups leaving out the same tilt
+    # share one kernel (computed once per distinct weight set of a batch);
+    # each left-out solve equals a Toeplitz plan built without the tilt, and
+    # stays within the parity bar of the NUFFT sweep.
+    from feilab_b200 import tools
+    z = golden["cli"]
+    args = (z["rows"], int(z["thickness"]), z["tilts"], tuple(int(v) for v in z["sched"]), int(z["data_type"]),
+            float(z["threshold"]))
+    frc_t, rp_t, _ = tools.loo_sweep(*args, capacity=capacity, operator="toeplitz")
+    _, rp_n, _ = tools.loo_sweep(*args, capacity=capacity)
+    nz = len(z["tilts"])
+    for omit in (0, nz // 2, nz - 1):
+        assert rel_l2(rp_t[omit], _reduced_plan_reprojection(z, omit, "toeplitz")) < 1e-6, omit
+        assert rel_l2(rp_t[omit], rp_n[omit]) < TOL_SOLVE, omit
+    assert np.all(np.isfinite(frc_t))
+
+
+def test_groups_with_equal_weights_share_a_toeplitz_kernel(golden):
+    # Per-group weights where several groups carry the same vector: the
+    # Toeplitz solve equals the one with the plan's own weights for those
+    # groups, and zero weights still remove the data term.
+    import torch
+    from feilab_b200.icon import IconPlan, weights
+    z = golden["a"]
+    rows_np = np.concatenate([z["rows"]] * 4)     # 12 slices: two groups of 8
+    S = rows_np.shape[0]
+    p = IconPlan(int(z["nx"]), int(z["thickness"]), z["tilts"], capacity=S)
+    p.set_operator("toeplitz")
+    rows = torch.from_numpy(np.ascontiguousarray(rows_np)).cuda()
+    sched = tuple(int(v) for v in z["sched"])
+    plain = p.solve(p.prepare_rhs(rows), sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+    G = (S + p.B - 1) // p.B
+    w = weights(int(z["nx"]), z["tilts"]).ravel()
+    p.set_group_weights(np.stack([w] * G))
+    same = p.solve(p.prepare_rhs(rows), sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+    assert np.array_equal(same, plain)
+    assert G >= 2
+    if G >= 2:
+        ws = np.stack([np.zeros_like(w)] + [w] * (G - 1))
+        p.set_group_weights(ws)
+        mixed = p.solve(p.prepare_rhs(rows), sched, int(z["data_type"]), float(z["threshold"])).cpu().numpy()
+        assert not np.any(mixed[:p.B]) and np.array_equal(mixed[p.B:], plain[p.B:])
+    p.close()

@@ -59,6 +59,9 @@ def _exact_iteration(o, w, m0, Ahwb):
     (64, 48, np.arange(-60, 61, 4)),
     (100, 9, np.linspace(-70, 70, 29)),
     (8, 8, np.array([-30.0, 0.0, 30.0])),
+    (48, 70, np.linspace(-60, 60, 15)),      # y-transforms of 192 = 32 x 6 points
+    (40, 150, np.linspace(-55, 50, 13)),     # 320 = 32 x 10
+    (33, 300, np.linspace(-60, 60, 9)),      # 640 = 32 x 20
 ])
 def test_toeplitz_iteration_matches_exact_transform(nx, th, tilts):
     from feilab_b200 import icon
@@ -151,10 +154,16 @@ def test_toeplitz_per_group_weights_equal_separate_plans(golden):
 
 
 @pytest.mark.parametrize("nx,th,ntilt", [
-    (1024, 160, 31),    # 8-slice groups, 512-point y transforms
-    (512, 257, 21),     # 8-slice groups, 1024-point y transforms
-    (2048, 200, 21),    # 4-slice groups (oversampled width 4096)
-    (4096, 100, 11),    # 2-slice groups (oversampled width 8192), 256-point y transforms
+    (1024, 160, 31),    # 8-slice groups, 320-point y transforms (R = 10)
+    (512, 257, 21),     # 8-slice groups, 640-point y transforms (R = 20)
+    (2048, 200, 21),    # 4-slice groups (oversampled width 4096), 512-point y transforms
+    (4096, 100, 11),    # 2-slice groups (oversampled width 8192), 256-point y transforms (R = 8)
+    (256, 80, 21),      # 192-point y transforms (R = 6)
+    (384, 180, 21),     # 384 (R = 12)
+    (1024, 300, 61),    # the production shape: 640 (R = 20)
+    (512, 350, 21),     # 768 (R = 24)
+    (512, 500, 21),     # 1024 (R = 32)
+    (256, 60, 21),      # 128 (R = 4)
 ])
 def test_toeplitz_iteration_matches_nufft_iteration_at_large_shapes(nx, th, ntilt):
     # One iteration from a random start with both normal operators: they are

@@ -225,6 +225,37 @@ def test_network_gradients_match_autograd():
         assert cos > TOL_GRAD_COS, (k, cos)
 
 
+TOL_GRAD_REL = 1e-1       # per-layer relative L2 of library gradients against the CPU fp32 mirror
+TOL_GRAD_ELEM = 2e-1      # every element within this fraction of the layer's largest reference gradient
+
+
+def test_network_gradients_match_cpu_fp32_mirror():
+    """The library's gradients (BF16 activations, FP32 accumulation on the
+    tensor cores) against autograd of the fp32 mirror run on the CPU, with
+    element-wise bounds per layer."""
+    plan, net, Ahwb = _net_case(seed=17)
+    p, gain = net.get_params()
+    g = torch.Generator(device="cuda").manual_seed(19)
+    target = torch.randn(Ahwb.shape, generator=g, device="cuda").contiguous()
+    loss = net.backprop(Ahwb, target)
+    grads = _split_params(torch.from_numpy(net.grads()))
+    A = Ahwb.cpu()
+    pt = torch.from_numpy(p).requires_grad_(True)
+    _, y, sc, _ = _mirror(pt, A, gain)
+    S, N0, N1 = A.shape
+    t = target.cpu().transpose(1, 2) / (sc[:, None, None] * gain)
+    ref_loss = ((y[:, :N1, :N0] - t) ** 2).mean()
+    ref_loss.backward()
+    assert abs(loss - ref_loss.item()) <= 2e-2 * ref_loss.item()
+    ref = _split_params(pt.grad.detach())
+    for k in ref:
+        a, b = grads[k].double(), ref[k].double()
+        rel = ((a - b).norm() / b.norm().clamp_min(1e-30)).item()
+        emax = (a - b).abs().max().item()
+        assert rel < TOL_GRAD_REL, (k, rel, emax / max(b.abs().max().item(), 1e-30))
+        assert emax <= TOL_GRAD_ELEM * b.abs().max().item() + 1e-12, (k, rel, emax, b.abs().max().item())
+
+
 def test_network_training_reduces_loss():
     plan, net, Ahwb = _net_case(seed=13)
     # A target the network can represent: a smoothed copy of its input.
