@@ -515,7 +515,8 @@ def run_ours(args):
             line["window_kb4"]["parity"] = {
                 op: parity_leg(lambda n: icon.IconPlan(NX, THICK, tilts, capacity=n, device=local, window="kb4"), op)
                 for op in ops}
-    line["warm_start"] = warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S)
+    if not args.no_warm:
+        line["warm_start"] = warm_start_leg(args, plan, rows, stream, barrier, max_over_ranks, world, S)
     if rank == 0:
         line["parity"] = {op: parity_leg(lambda n: icon.IconPlan(NX, THICK, tilts, capacity=n, device=local), op)
                           for op in ops}
@@ -792,6 +793,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference ICON-GPU leg")
     ap.add_argument("--no-kb", action="store_true", help="skip the Kaiser-Bessel window leg")
+    ap.add_argument("--no-warm", action="store_true", help="skip the warm-start leg")
     ap.add_argument("--operator", default="toeplitz", choices=["nufft", "toeplitz"],
                     help="normal operator of the headline run (the other is timed beside it)")
     ap.add_argument("--uneven-scale", type=float, default=0.25,

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -263,6 +264,13 @@ struct icon_plan {
     // iteration's update m -= alpha Re r-hat into the next iteration's forward
     // x-pass; flush_update applies a pending one where the loop ends.
     bool xt_ok = false;         // k_xtoep has a variant for n0
+    // TMA staging of the x-kernels' columns: tensor maps over G1, Ahwb, r-hat
+    // and m (xt_tma), boxes of xt_bh slices; device error flag of their
+    // bounded waits.
+    bool xt_tma = false, xt_tma_m = false;
+    int xt_bh = 1, xt_box_g1 = 0, xt_box_img = 0;
+    CUtensorMap tm_g1, tm_ahwb, tm_rhat, tm_m;
+    int *dev_err = nullptr;
     bool upd_pending = false, upd_clamp = false;
     int upd_dtype = 0, upd_G = 0;
     float upd_thr = 0.f;
@@ -333,6 +341,21 @@ struct icon_plan {
         g.tw1 = tw1t;
         return g;
     }
+    // The TMA part of the x-kernels' arguments.
+    void fill_xt(icon::XtArgs &xa) const
+    {
+        xa.use_tma = xt_tma ? 1 : 0;
+        xa.tma_m = xt_tma_m ? 1 : 0;
+        xa.box_g1 = xt_box_g1;
+        xa.box_img = xt_box_img;
+        xa.err = dev_err;
+        if (xt_tma) {
+            xa.tm_g1 = tm_g1;
+            xa.tm_ahwb = tm_ahwb;
+            xa.tm_rhat = tm_rhat;
+            xa.tm_m = tm_m;
+        }
+    }
     Geo1 geo1() const
     {
         Geo1 g;
@@ -391,6 +414,77 @@ struct DeviceGuard {
         if (prev >= 0 && cur != prev) cudaSetDevice(prev);
     }
 };
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled()
+{
+    static std::once_flag once;
+    static EncodeTiledFn fn = nullptr;
+    std::call_once(once, [] {
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(ptr);
+    });
+    return fn;
+}
+
+// A FP32 tensor map of rank dims (innermost first), strides in bytes of
+// dims 1.., box extents; no swizzle, no interleave, zero fill outside.
+bool make_map(CUtensorMap *m, void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
+              const cuuint32_t *box)
+{
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    const cuuint32_t es[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, base, dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor maps for the x-kernels' TMA staging (k_xtoep): possible when a CTA
+// takes at least 2 slices (boxes of 16 bytes or more, every coordinate and
+// stride a multiple of 16 bytes); m needs 4.  ICON_XT_TMA=0 keeps the
+// per-thread cp.async staging.
+void setup_xt_tma(icon_plan *p)
+{
+    const int n0 = p->n0, B = p->B;
+    p->xt_bh = n0 <= 1024 ? B : n0 == 2048 ? std::min(B, 4) : n0 == 4096 ? std::min(B, 2) : 1;
+    const char *env = std::getenv("ICON_XT_TMA");
+    if (!p->xt_ok || p->xt_bh < 2 || (env && env[0] == '0')) return;
+    const int BH = p->xt_bh;
+    p->xt_box_g1 = std::min(256, n0);
+    p->xt_box_img = std::min(256, n0 / 2);
+    const cuuint64_t G = (cuuint64_t)p->Gcap, N0 = (cuuint64_t)p->N0, N1 = (cuuint64_t)p->N1, Bz = (cuuint64_t)B;
+    bool ok = true;
+    {   // G1 [Gcap n0][N1 B 2] floats
+        const cuuint64_t dims[2] = {N1 * Bz * 2, G * (cuuint64_t)n0};
+        const cuuint64_t str[1] = {N1 * Bz * 8};
+        const cuuint32_t box[2] = {(cuuint32_t)(BH * 2), (cuuint32_t)p->xt_box_g1};
+        ok = ok && make_map(&p->tm_g1, p->G1, 2, dims, str, box);
+    }
+    {   // Ahwb and r-hat [Gcap N1][N0][B 2] floats
+        const cuuint64_t dims[3] = {Bz * 2, N0, G * N1};
+        const cuuint64_t str[2] = {Bz * 8, N0 * Bz * 8};
+        const cuuint32_t box[3] = {(cuuint32_t)(BH * 2), (cuuint32_t)p->xt_box_img, 1};
+        ok = ok && make_map(&p->tm_ahwb, p->Ahwb, 3, dims, str, box);
+        ok = ok && make_map(&p->tm_rhat, p->rhat, 3, dims, str, box);
+    }
+    bool ok_m = BH >= 4;
+    if (ok_m) {   // m [Gcap N1][N0][B] floats
+        const cuuint64_t dims[3] = {Bz, N0, G * N1};
+        const cuuint64_t str[2] = {Bz * 4, N0 * Bz * 4};
+        const cuuint32_t box[3] = {(cuuint32_t)BH, (cuuint32_t)p->xt_box_img, 1};
+        ok_m = make_map(&p->tm_m, p->m, 3, dims, str, box);
+    }
+    p->xt_tma = ok;
+    p->xt_tma_m = ok && ok_m;
+}
 
 // Builds window tables and the per-row entry lists of M nodes at xy.
 icon_status build_tables(icon_plan *p, const float *xy, const float *w, int M, NodeTables &t)
@@ -546,6 +640,7 @@ icon_status launch_adjoint(icon_plan *p, const float2 *f_int, int G, int mode, f
     dim3 gy(G, p->n0), gx(p->N1, G);
     size_t smem = p->smem_x + sizeof(double) * p->thr_x;
     icon::XtArgs xa{};
+    p->fill_xt(xa);
     xa.N0 = p->N0; xa.N1 = p->N1; xa.n0 = p->n0; xa.tw0 = p->tw0; xa.G1 = p->G1; xa.rhat = out_int;
     xa.Ahwb = p->Ahwb; xa.part_rtr = p->part_rtr; xa.rcx = p->rcx; xa.rcy = p->rcy; xa.resid = mode == 0 ? 0 : 1;
     WITH_B(p->B,
@@ -666,6 +761,7 @@ icon_status launch_iteration_xt_raw(icon_plan *p, int G, bool upd, bool clamp_pr
     const double slots = (double)G * p->B;
     const double NN = (double)p->N0 * p->N1, G1b = (double)p->n0 * p->N1 * 8, Kb = (double)p->n0 * p->n1t * 4;
     icon::XtArgs xa{};
+    p->fill_xt(xa);
     xa.N0 = p->N0; xa.N1 = p->N1; xa.n0 = p->n0; xa.tw0 = p->tw0; xa.G1 = p->G1; xa.m = p->m;
     xa.rhat_in = p->rhat; xa.alpha = p->alpha; xa.upd = upd ? 1 : 0; xa.clamp = clamp_prev ? 1 : 0;
     xa.data_type = data_type; xa.thr = thr; xa.rhat = p->rhat; xa.Ahwb = p->Ahwb; xa.part_rtr = p->part_rtr;
@@ -1023,6 +1119,9 @@ static icon_status plan_create_impl(const icon_geometry *geo, int group, icon_pl
     ICON_TRY(p->arena.alloc(&p->alpha, G * Bz));
     ICON_TRY(p->arena.alloc(&p->step_part, G * 512 * Bz * 2));
     ICON_TRY(p->arena.alloc(&p->step, G * Bz));
+    ICON_TRY(p->arena.alloc(&p->dev_err, 1));
+    ICON_CUDA(cudaMemset(p->dev_err, 0, sizeof(int)));
+    setup_xt_tma(p.get());
     ICON_CUDA(cudaDeviceSynchronize());
     *out = p.release();
     return ICON_OK;
@@ -1545,6 +1644,16 @@ icon_status icon_trace_read(icon_plan *p, int *h_count, double *h_ms, double *h_
 }
 
 long long icon_launch_count(const icon_plan *p) { return p ? p->launches : 0; }
+
+icon_status icon_plan_device_error(icon_plan *p, int *h_code)
+{
+    if (!p || !h_code) return fail(ICON_ERR_INVALID, "null argument");
+    DeviceGuard guard(p->dev);
+    ICON_CUDA(cudaDeviceSynchronize());
+    ICON_CUDA(cudaMemcpy(h_code, p->dev_err, sizeof(int), cudaMemcpyDeviceToHost));
+    ICON_CUDA(cudaMemset(p->dev_err, 0, sizeof(int)));
+    return ICON_OK;
+}
 
 }  // extern "C"
 

@@ -31,6 +31,7 @@
 // output times (-1)^k.
 #pragma once
 #include "icon_device.cuh"
+#include "ws_tc.cuh"
 
 namespace icon {
 
@@ -1493,7 +1494,26 @@ struct XtArgs {
     double *part_rtr;        // mid / adjoint with resid: [G][N1][B] partial |r-hat|^2 per column
     const float *rcx, *rcy;  // adjoint: deapodisation reciprocals 1/cx [N0], 1/cy [N1]
     int resid;               // adjoint: subtract Ahwb and sum |.|^2 (else the plain adjoint)
+    // TMA staging of the columns (use_tma; BH >= 2): the plan's G1 as 2-D
+    // [Gcap n0 rows][N1 B 2 floats], its Ahwb and r-hat as 3-D
+    // [Gcap N1][N0][B 2 floats], and (tma_m; BH >= 4) its m as
+    // [Gcap N1][N0][B floats]; boxes of BH slices by box_g1 / box_img rows.
+    // Every wait on the loads is bounded and reports through err.
+    CUtensorMap tm_g1, tm_ahwb, tm_rhat, tm_m;
+    int use_tma, tma_m, box_g1, box_img;
+    int *err;
 };
+
+// Bounded wait of all threads of a CTA on a TMA barrier; false (the same in
+// every thread) when any thread's wait ran out, after recording the error
+// and giving the loads a second bounded wait to land.
+__device__ __forceinline__ bool xt_tma_wait(uint64_t *bar, int *err)
+{
+    bool ok = ws::mbar_wait(bar, 0, err, ws::kErrLoadWait);
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok) ws::mbar_wait(bar, 0, err, ws::kErrLoadWait);
+    return ok;
+}
 
 template <int BH, int LA, int LNB>
 struct XtShape {
@@ -1662,11 +1682,14 @@ __device__ __forceinline__ void xt_inverse(float2 (&v)[32 >> LA][1 << LA], float
 // fastest.
 template <int B, int BH, int LA, int LNB, int MODE>
 __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>::T >= 256) ? 2 : 4)
-    k_xtoep(XtArgs g)
+    k_xtoep(const __grid_constant__ XtArgs g)
 {
     using S = XtShape<BH, LA, LNB>;
     constexpr int NA = S::NA, NB = S::NB, U = S::U, H = B / BH;
-    extern __shared__ float2 s[];
+    extern __shared__ __align__(128) float2 s[];
+    __shared__ __align__(8) uint64_t bar[2];   // TMA: [0] the G1 or m column, [1] the Ahwb or r-hat column
+    constexpr bool kTma = BH >= 2;
+    const bool tma = kTma && g.use_tma;
     double *red = reinterpret_cast<double *>(s + S::N * BH);
     const int Y = blockIdx.x / H, h = blockIdx.x % H, grp = blockIdx.y;
     const int t = threadIdx.x, sl = t % BH, u = t / BH, bsl = h * BH + sl;   // bsl: slice within the group
@@ -1675,8 +1698,34 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
     float2 *col = g.G1 + ((size_t)grp * n * N1 + Y) * B + bsl;       // row x at col[x * rstride]
     const size_t ibase = ((size_t)grp * N1 + Y) * N0 * B + bsl;        // image point X at ibase + X*B
     float2 v[S::NI1][NA];
-    float2 *As = s + S::N * BH + S::T;   // mid: this CTA's Ahwb column, [N0][BH]
-    if constexpr (MODE >= 1) {
+    // mid: this CTA's Ahwb column, [N0][BH], at a 128-byte boundary (a TMA destination)
+    float2 *As = s + ((S::N * BH + S::T + 15) & ~15);
+    if (tma) {
+        if (t == 0) {
+            ws::mbar_init(&bar[0], 1);
+            ws::mbar_init(&bar[1], 1);
+            ws::mbar_fence_init();
+        }
+        __syncthreads();
+    }
+    if (MODE >= 1 && tma) {
+        // One thread issues the column's loads: the G1 column in boxes of
+        // box_g1 rows x BH values into s as [x][BH], then the Ahwb column in
+        // boxes of box_img points into As (rows past N0 read as zeros and
+        // land inside As, whose n0/2 rows are a multiple of the box).
+        if (t == 0) {
+            ws::mbar_expect_tx(&bar[0], (uint32_t)(n * BH * sizeof(float2)));
+            for (int x0 = 0; x0 < n; x0 += g.box_g1)
+                ws::tma_load_2d(s + x0 * BH, &g.tm_g1, (Y * B + h * BH) * 2, grp * n + x0, &bar[0]);
+            if (MODE == 1 || g.resid) {
+                const int nbox = (N0 + g.box_img - 1) / g.box_img;
+                ws::mbar_expect_tx(&bar[1], (uint32_t)(nbox * g.box_img * BH * sizeof(float2)));
+                for (int k = 0; k < nbox; ++k)
+                    ws::tma_load_3d(As + k * g.box_img * BH, &g.tm_ahwb, h * BH * 2, k * g.box_img, grp * N1 + Y,
+                                    &bar[1]);
+            }
+        }
+    } else if constexpr (MODE >= 1) {
         // The G1 column (n0 rows of BH values, rows N1*B float2 apart) into s
         // as [x][BH], then the Ahwb column, staged while the inverse runs.
         const float2 *gsrc = g.G1 + ((size_t)grp * n * N1 + Y) * B + h * BH;
@@ -1708,7 +1757,24 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
         // The m column (N0 x BH floats) into s and, for the update, the r-hat
         // column into As, by cp.async; then into registers.
         float *Ms = reinterpret_cast<float *>(s);
-        {
+        if (tma && g.tma_m) {
+            // m and (for the update) the r-hat column by TMA, boxes of
+            // box_img points: m as [X][BH] floats into s, r-hat into As.
+            const int nbox = (N0 + g.box_img - 1) / g.box_img;
+            if (t == 0) {
+                ws::mbar_expect_tx(&bar[0], (uint32_t)(nbox * g.box_img * BH * sizeof(float)));
+                for (int k = 0; k < nbox; ++k)
+                    ws::tma_load_3d(Ms + k * g.box_img * BH, &g.tm_m, h * BH, k * g.box_img, grp * N1 + Y, &bar[0]);
+                if (g.upd) {
+                    ws::mbar_expect_tx(&bar[1], (uint32_t)(nbox * g.box_img * BH * sizeof(float2)));
+                    for (int k = 0; k < nbox; ++k)
+                        ws::tma_load_3d(As + k * g.box_img * BH, &g.tm_rhat, h * BH * 2, k * g.box_img,
+                                        grp * N1 + Y, &bar[1]);
+                }
+            }
+            if (!xt_tma_wait(&bar[0], g.err)) return;
+            if (g.upd && !xt_tma_wait(&bar[1], g.err)) return;
+        } else {
             const float *msrc = g.m + ibase - sl;           // point X of this CTA's slices at msrc + X*B
             const float2 *rsrc = g.rhat_in + ibase - sl;
             for (int X = t; X < N0; X += S::T) {
@@ -1764,11 +1830,20 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
         __syncthreads();   // the staged m is read before step 1 rewrites s
         xt_forward<BH, LA, LNB>(v, s, u, sl, g.tw0, col, rstride);
     } else if constexpr (MODE == 2) {
-        cp_async_wait<1>();
-        __syncthreads();
+        if (tma) {
+            if (!xt_tma_wait(&bar[0], g.err)) return;
+        } else {
+            cp_async_wait<1>();
+            __syncthreads();
+        }
         xt_inverse<BH, LA, LNB>(v, s, u, sl, g.tw0);
-        cp_async_wait<0>();
-        __syncthreads();
+        if (tma) {
+            if (g.resid && !xt_tma_wait(&bar[1], g.err)) return;
+            __syncthreads();
+        } else {
+            cp_async_wait<0>();
+            __syncthreads();
+        }
         const float rcyY = g.rcy[Y];
         double acc = 0.0;
 #pragma unroll
@@ -1800,11 +1875,20 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
             if (t < BH) g.part_rtr[((size_t)grp * N1 + Y) * B + h * BH + t] = red[t];
         }
     } else {
-        cp_async_wait<1>();    // the column group (Ahwb may still be landing)
-        __syncthreads();
+        if (tma) {
+            if (!xt_tma_wait(&bar[0], g.err)) return;
+        } else {
+            cp_async_wait<1>();    // the column group (Ahwb may still be landing)
+            __syncthreads();
+        }
         xt_inverse<BH, LA, LNB>(v, s, u, sl, g.tw0);
-        cp_async_wait<0>();
-        __syncthreads();   // Ahwb staged; every read of s by the inverse is done
+        if (tma) {
+            if (!xt_tma_wait(&bar[1], g.err)) return;
+            __syncthreads();   // every read of s by the inverse is done
+        } else {
+            cp_async_wait<0>();
+            __syncthreads();   // Ahwb staged; every read of s by the inverse is done
+        }
         double acc = 0.0;
 #pragma unroll
         for (int i = 0; i < S::NI1; ++i) {
@@ -1839,7 +1923,7 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
 // and (mid) the staged Ahwb column of N0 <= n0 / 2 points.
 __host__ __device__ inline size_t xtoep_smem(int n0, int BH)
 {
-    return (size_t)n0 * BH * sizeof(float2) + (size_t)(n0 * BH / 32) * sizeof(double) +
+    return (size_t)n0 * BH * sizeof(float2) + (size_t)(n0 * BH / 32) * sizeof(double) + 128 +
            (size_t)(n0 / 2) * BH * sizeof(float2);
 }
 

@@ -69,6 +69,7 @@ def lib():
         L.icon_trace_read.argtypes = [P, V, V, V]
         L.icon_launch_count.argtypes = [P]
         L.icon_launch_count.restype = ctypes.c_longlong
+        L.icon_plan_device_error.argtypes = [P, ctypes.POINTER(I)]
         L.icon_last_error.restype = ctypes.c_char_p
         for name in ("icon_plan_create", "icon_plan_destroy", "icon_plan_query", "icon_plan_geometry",
                      "icon_nufft_forward", "icon_nufft_forward_complex", "icon_nufft_adjoint",
@@ -77,7 +78,8 @@ def lib():
                      "icon_reconstruct_stack", "icon_reconstruct_stack_host", "icon_host_alloc", "icon_host_free",
                      "icon_stack_upload", "icon_device_free", "icon_weights", "icon_plan_set_group_weights",
                      "icon_plan_set_operator", "icon_plan_set_stop", "icon_reproject_host", "icon_batch_create",
-                     "icon_batch_destroy", "icon_batch_tuning", "icon_batch_reconstruct_host"):
+                     "icon_batch_destroy", "icon_batch_tuning", "icon_batch_reconstruct_host",
+                     "icon_plan_device_error"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -404,6 +406,13 @@ class IconPlan:
         _check(lib().icon_trace_read(self._h, ctypes.cast(cnt, ctypes.c_void_p), ctypes.cast(ms, ctypes.c_void_p),
                                      ctypes.cast(by, ctypes.c_void_p)))
         return {k: (int(cnt[i]), float(ms[i]), float(by[i])) for i, k in enumerate(self.TRACE_KINDS)}
+
+    def device_error(self):
+        """Reads and clears the plan's device error flag (0: none; 1: a
+        bounded wait for the x-kernels' TMA loads ran out)."""
+        v = ctypes.c_int(0)
+        _check(lib().icon_plan_device_error(self._h, ctypes.byref(v)))
+        return int(v.value)
 
     def launch_count(self):
         return int(lib().icon_launch_count(self._h))

@@ -152,6 +152,19 @@ def add_noise(rows: torch.Tensor, snr: float, seed: int) -> torch.Tensor:
     return rows + noise * math.sqrt(var / snr)
 
 
+def cfg2_kind(nx, ny, thickness, seed, ys=None, device="cpu"):
+    """A tilt series of the 1024x1024x300 kind at another size: ellipsoids
+    and Gaussian blobs at the production phantom's density per voxel (300 and
+    3000 per 1024 x 1024 x 300 voxels), background 0.1, 61 tilts -60..60 step
+    2, SNR 0.1.  Returns (rows (S, 61, nx), tilts)."""
+    vol = nx * ny * thickness / (1024.0 * 1024.0 * 300.0)
+    tilts = tilt_angles(-60, 60, 2)
+    ph = make_phantom((nx, ny, thickness), max(1, round(300 * vol)), max(1, round(3000 * vol)), seed=seed,
+                      background=0.1)
+    rows = project(ph, tilts, ys=ys, device=device)
+    return add_noise(rows, 0.1, seed), tilts
+
+
 def series(config: str, device="cpu", ys=None, seed=None):
     """Named workloads.  Returns (rows (S, ntilt, nx) float32 tensor, tilts,
     thickness, description).

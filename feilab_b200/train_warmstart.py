@@ -1,6 +1,8 @@
 """Train the warm-start network for one geometry on synthetic tilt series.
 
     python -m feilab_b200.train_warmstart --out feilab_b200/weights/warmstart_1024x300.npz
+    python -m feilab_b200.train_warmstart --nx 512 --thickness 256 --seeds 20 --per-seed 1000 \
+        --schedule 10,480,10 --batch 32 --epochs 20 --heldout 1024 --out feilab_b200/weights/warmstart_512x256.npz
 
 Training slices come from phantoms of the 1024x1024x300 / 61-tilt kind
 (300 ellipsoids + 3000 Gaussian blobs on a 0.1 background, SNR 0.1) with
@@ -26,13 +28,19 @@ import numpy as np
 
 
 def make_data(plan, seeds, per_seed, sched, data_type, threshold, batch, log):
+    """Inputs A^H W b and plain-ICON targets of per_seed slices of each
+    phantom: the 1024x1024x300 series itself at that size, else a phantom of
+    its kind with plan.N0 x per_seed x plan.N1 voxels."""
     import torch
     from . import synth
     As, Ms = [], []
     for sd in seeds:
-        g = np.random.default_rng(sd)
-        ys = sorted(g.choice(1024, size=per_seed, replace=False).tolist())
-        rows, tilts, th, _ = synth.series("cfg2", device="cuda", ys=ys, seed=sd)
+        if (plan.N0, plan.N1) == (1024, 300):
+            g = np.random.default_rng(sd)
+            ys = sorted(g.choice(1024, size=per_seed, replace=False).tolist())
+            rows, tilts, th, _ = synth.series("cfg2", device="cuda", ys=ys, seed=sd)
+        else:
+            rows, tilts = synth.cfg2_kind(plan.N0, per_seed, plan.N1, sd, device="cuda")
         for s0 in range(0, per_seed, batch):
             r = rows[s0:s0 + batch].contiguous()
             A = plan.prepare_rhs(r)
@@ -87,6 +95,9 @@ def main(argv=None):
     ap.add_argument("--eval-only", default=None, help="load weights from this file instead of training")
     ap.add_argument("--heldout", type=int, default=64, help="held-out slices")
     ap.add_argument("--log", default=None)
+    ap.add_argument("--nx", type=int, default=1024)
+    ap.add_argument("--thickness", type=int, default=300)
+    ap.add_argument("--schedule", default="10,280,10", help="schedule of the target solves")
     args = ap.parse_args(argv)
 
     import torch
@@ -101,9 +112,10 @@ def main(argv=None):
             logf.write(line + "\n")
             logf.flush()
 
-    sched, data_type, threshold = (10, 280, 10), 2, 0.0
+    sched, data_type, threshold = tuple(int(v) for v in args.schedule.split(",")), 2, 0.0
     tilts = synth.tilt_angles(-60, 60, 2)
-    plan = icon.IconPlan(1024, 300, tilts, capacity=128)
+    plan = icon.IconPlan(args.nx, args.thickness, tilts, capacity=128)
+    plan.set_operator("toeplitz")
     t0 = time.time()
     A, M = make_data(plan, [5001 + k for k in range(args.seeds)], args.per_seed, sched, data_type, threshold, 128, log)
     Ah, Mh = make_data(plan, [9001], args.heldout, sched, data_type, threshold, 64, log)
@@ -161,7 +173,7 @@ def main(argv=None):
     # (a, k, c) after which the result has FRC >= 0.99 against the full cold
     # solve (a, b, c), for cold and warm starts.
     curve = []
-    for k in (0, 10, 20, 40, 70, 100, 150, 200, 280):
+    for k in [k for k in (0, 10, 20, 40, 70, 100, 150, 200, 280, 380, 480) if k <= b]:
         mc = plan.solve(hb, (a, k, c), data_type, threshold)
         mw = plan.solve(hb, (a, k, c), data_type, threshold, m0=m0)
         fc, fw = frc_mean(mc, m_cold), frc_mean(mw, m_cold)
@@ -178,13 +190,46 @@ def main(argv=None):
     k_cold = next((k for k, fc, fw in curve if fc >= 0.99), b)
     k_warm = next((k for k, fc, fw in curve if fw >= 0.99), b)
     log(f"  ICON iterations to FRC >= 0.99: cold {k_cold}, warm {k_warm}")
+    # Every held-out slice to the tolerance: cold (icon_solve_until from
+    # m = 0) against warm (network start, icon_solve_warm with its acceptance
+    # test and cold redo), device-timed, FRC against the full cold solve.
+    full = {}
+    cap = plan.capacity
+    for name in ("cold", "warm"):
+        its, redone, frcs = [], 0, []
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        outs = []
+        for s0 in range(0, Ah.shape[0], cap):
+            a = Ah[s0:s0 + cap].contiguous()
+            if name == "cold":
+                m, it, _ = plan.solve_until(a, tol, sched, data_type, threshold, check_every=10)
+            else:
+                m0 = torch.empty_like(a.real).contiguous()
+                for q in range(0, a.shape[0], args.batch):
+                    net.predict(a[q:q + args.batch].contiguous(), out=m0[q:q + args.batch])
+                m, why, it = plan.solve_warm(a, m0, tol, sched, data_type, threshold, check_every=10)
+                redone += int((why != 0).sum())
+            its.append(it)
+            outs.append(m)
+        e1.record()
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        for q, m in enumerate(outs):
+            frcs.append(frc_mean(m, Mh[q * cap:q * cap + m.shape[0]]))
+        frcs = np.concatenate(frcs)
+        full[name] = dict(slices_per_s=float(Ah.shape[0] / sec), iterations=its, redone_cold=redone,
+                          frc_vs_full_cold_min=float(frcs.min()), frc_vs_full_cold_median=float(np.median(frcs)))
+        log(f"  all {Ah.shape[0]} held-out slices to tolerance {tol:g}, {name}: {full[name]}")
     params, g = net.get_params()
-    meta = dict(nx=1024, thickness=300, tilts="-60..60 step 2", schedule=list(sched), data_type=data_type,
+    meta = dict(nx=args.nx, thickness=args.thickness, tilts="-60..60 step 2", schedule=list(sched), data_type=data_type,
                 threshold=threshold, train_slices=int(n), epochs=args.epochs, batch=args.batch, lr=args.lr,
                 heldout_rel_error=float(np.median(err)), heldout_tol=tol, heldout_iters_cold=n_cold,
                 heldout_iters_warm=n_warm, heldout_frc_min=float(frc.min()), frc_curve=curve,
                 icon_iters_to_frc099_cold=k_cold, icon_iters_to_frc099_warm=k_warm,
-                prediction_frc_min=float(f0.min()), frc_curve_warm_no_first_infr=curve0)
+                prediction_frc_min=float(f0.min()), frc_curve_warm_no_first_infr=curve0, heldout_slices=int(Ah.shape[0]),
+                heldout_to_tol=full)
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     np.savez(args.out, params=params, gain=np.float32(g), meta=json.dumps(meta))
     log(f"saved {args.out}: {json.dumps(meta)}")

@@ -337,6 +337,12 @@ icon_status icon_trace_read(icon_plan *plan, int *h_count, double *h_ms, double 
 /* Number of kernels this plan has launched since it was created. */
 long long icon_launch_count(const icon_plan *plan);
 
+/* Reads and clears the plan's device error flag: 0, or 1 when a bounded wait
+ * of the x-kernels for their TMA column loads ran out (the kernel then
+ * skipped its output, so results since the last read are not valid).
+ * Synchronises the device.  No counterpart in the reference. */
+icon_status icon_plan_device_error(icon_plan *plan, int *h_code);
+
 /* icon_rows_forward_noalloc: the work of icon_rows_forward (the 1-D NUFFT of
  * every projection row, d_b[S][ntilt*nx] complex) for callers that cannot
  * allocate device memory -- a process whose own pool allocator owns all

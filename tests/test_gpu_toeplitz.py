@@ -188,3 +188,29 @@ def test_toeplitz_iteration_matches_nufft_iteration_at_large_shapes(nx, th, ntil
         assert abs(alt[0, s] - aln[0, s]) <= TOL_STAGE * abs(aln[0, s])
         assert abs(rtt[0, s] - rtn[0, s]) <= TOL_STAGE * abs(rtn[0, s])
     p.close()
+
+
+@pytest.mark.parametrize("nx,th,S", [(1024, 300, 16), (2048, 400, 8), (512, 257, 16), (64, 40, 2)])
+def test_tma_column_staging_is_bit_identical(nx, th, S, monkeypatch):
+    # The x-kernels stage their G1, Ahwb, r-hat and m columns by TMA (tensor
+    # maps, one thread issuing the loads, bounded mbarrier waits) where a CTA
+    # takes two or more slices; ICON_XT_TMA=0 keeps the per-thread cp.async
+    # staging.  The arithmetic is the same, so the results are equal bit for
+    # bit, for both operators' x-kernels (the NUFFT adjoint's last x-pass and
+    # the Toeplitz iteration's), and no wait runs out.
+    from feilab_b200 import icon
+    tilts = np.linspace(-60, 60, 31).astype(np.float32)
+    rng = np.random.default_rng(nx + th)
+    rows = rng.standard_normal((S, len(tilts), nx)).astype(np.float32)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("ICON_XT_TMA", flag)
+        p = icon.IconPlan(nx, th, tilts, capacity=S)
+        p.set_operator("toeplitz")
+        A = p.prepare_rhs(_t(rows))
+        m = p.solve(A, (2, 4, 2), 2, 0.0)
+        out[flag] = (A.cpu().numpy(), m.cpu().numpy())
+        assert p.device_error() == 0
+        p.close()
+    assert np.array_equal(out["1"][0], out["0"][0])
+    assert np.array_equal(out["1"][1], out["0"][1])
