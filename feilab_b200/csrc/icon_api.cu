@@ -267,6 +267,14 @@ struct icon_plan {
     // TMA staging of the x-kernels' columns: tensor maps over G1, Ahwb, r-hat
     // and m (xt_tma), boxes of xt_bh slices; device error flag of their
     // bounded waits.
+    // Warm start of the reconstruct calls (icon_plan_set_warm_start): the
+    // network, the acceptance test, caller-layout buffers of A^H W b and m,
+    // and counts of the slices accepted and redone from zero.
+    icon_ws *ws = nullptr;
+    icon_warm_cfg wcfg{};
+    float2 *ws_A = nullptr;
+    float *ws_m = nullptr;
+    long long warm_accepted = 0, warm_redone = 0;
     bool xt_tma = false, xt_tma_m = false;
     int xt_bh = 1, xt_box_g1 = 0, xt_box_img = 0;
     CUtensorMap tm_g1, tm_ahwb, tm_rhat, tm_m;
@@ -875,8 +883,11 @@ icon_status run_schedule_tol(icon_plan *p, const icon_solve_cfg *cfg, int G, int
 // After the row transform of G groups (Sc slices): Ahwb = A^H W b, m = 0,
 // the schedule's iterations (MainCode.cu:115-140 with Iteration3), ended at
 // the plan's tolerance when one is set (icon_plan_set_stop).
+icon_status solve_from_rows_warm(icon_plan *p, const icon_solve_cfg *cfg, int G, int Sc, cudaStream_t st);
+
 icon_status solve_from_rows(icon_plan *p, const icon_solve_cfg *cfg, int G, int Sc, cudaStream_t st)
 {
+    if (p->ws) return solve_from_rows_warm(p, cfg, G, Sc, st);
     const int a = cfg->infr_before, b = cfg->icon, c = cfg->infr_after, iters = a + b + c;
     ICON_TRY(ensure_toeplitz(p, st));
     ICON_TRY(launch_adjoint(p, p->f, G, 0, p->Ahwb, st));
@@ -887,6 +898,29 @@ icon_status solve_from_rows(icon_plan *p, const icon_solve_cfg *cfg, int G, int 
     for (int it = 0; it < iters; ++it)
         ICON_TRY(launch_iteration(p, G, a <= it && it < iters - c, cfg->data_type, cfg->threshold, nullptr, nullptr, st));
     return flush_update(p, st);
+}
+
+// The same with the plan's warm start: A^H W b in the caller layout, the
+// network's start, icon_solve_warm (its acceptance test and cold redo), the
+// result back in the plan's layout for the output stage.
+icon_status solve_from_rows_warm(icon_plan *p, const icon_solve_cfg *cfg, int G, int Sc, cudaStream_t st)
+{
+    ICON_TRY(ensure_toeplitz(p, st));
+    ICON_TRY(launch_adjoint(p, p->f, G, 0, p->Ahwb, st));
+    const size_t NN = (size_t)p->N0 * p->N1;
+    LAUNCH(p, K_LAYOUT, st, icon::k_img_out<float2><<<grid1d((size_t)Sc * NN), 256, 0, st>>>(p->Ahwb, p->ws_A, Sc, p->N0, p->N1, p->B));
+    ICON_CUDA(cudaGetLastError());
+    const int wcap = iconx::ws_capacity(p->ws);
+    for (int s0 = 0; s0 < Sc; s0 += wcap)
+        ICON_TRY(icon_ws_predict(p->ws, p->ws_A + s0 * NN, p->ws_m + s0 * NN, std::min(wcap, Sc - s0), st));
+    std::vector<int> why(Sc, 0);
+    int iters = 0;
+    ICON_TRY(icon_solve_warm(p, cfg, p->ws_A, p->ws_m, Sc, &p->wcfg, why.data(), &iters, st));
+    for (int s = 0; s < Sc; ++s) (why[s] == ICON_WARM_ACCEPTED ? p->warm_accepted : p->warm_redone)++;
+    const size_t tot = (size_t)G * p->N1 * p->N0 * p->B;
+    LAUNCH(p, K_LAYOUT, st, icon::k_img_in<float><<<grid1d(tot), 256, 0, st>>>(p->ws_m, p->m, Sc, p->N0, p->N1, p->B, tot));
+    ICON_CUDA(cudaGetLastError());
+    return ICON_OK;
 }
 
 icon_status line_tables(icon_plan *p, float tilt_deg, NodeTables **out)
@@ -1205,6 +1239,33 @@ icon_status icon_plan_set_group_weights(icon_plan *p, const float *h_w, int ngro
     p->kt_unique = (int)sets.size();
     p->wgroups = ngroups;
     p->kt_stale = true;
+    return ICON_OK;
+}
+
+icon_status icon_plan_set_warm_start(icon_plan *p, icon_ws *ws, const icon_warm_cfg *wc)
+{
+    if (!p) return fail(ICON_ERR_INVALID, "null plan");
+    if (!ws) {
+        p->ws = nullptr;
+        return ICON_OK;
+    }
+    if (!wc || !(wc->tol > 0.0) || wc->check_every < 1 || !(wc->max_dist > 0.0))
+        return fail(ICON_ERR_INVALID, "icon_plan_set_warm_start: tol > 0, check_every >= 1 and max_dist > 0 required");
+    if (iconx::ws_capacity(ws) < 1) return fail(ICON_ERR_INVALID, "icon_plan_set_warm_start: bad network");
+    DeviceGuard guard(p->dev);
+    const size_t NN = (size_t)p->N0 * p->N1;
+    if (!p->ws_A) ICON_TRY(p->arena.alloc(&p->ws_A, (size_t)p->cap * NN));
+    if (!p->ws_m) ICON_TRY(p->arena.alloc(&p->ws_m, (size_t)p->cap * NN));
+    p->ws = ws;
+    p->wcfg = *wc;
+    return ICON_OK;
+}
+
+icon_status icon_plan_warm_counts(const icon_plan *p, long long *h_accepted, long long *h_redone)
+{
+    if (!p) return fail(ICON_ERR_INVALID, "null plan");
+    if (h_accepted) *h_accepted = p->warm_accepted;
+    if (h_redone) *h_redone = p->warm_redone;
     return ICON_OK;
 }
 

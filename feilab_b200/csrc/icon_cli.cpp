@@ -25,6 +25,7 @@
 
 #include "icon_b200.h"
 #include "icon_tools.h"
+#include "icon_warmstart.h"
 #include "mrc_io.h"
 
 namespace {
@@ -51,7 +52,11 @@ void help()
            "    with this run's sizes; they are read back, not recomputed),\n"
            "  --window gauss6|kb4 (NUFFT window of the input stage, the reprojections and the NUFFT operator: the\n"
            "    Gaussian of half-width 6, default, or the Kaiser-Bessel window of half-width 4, 8 taps instead of 14;\n"
-           "    the leave-one-out sweep of --loo keeps the Gaussian)\n");
+           "    the leave-one-out sweep of --loo keeps the Gaussian),\n"
+           "  --warm-start FILE (start each slice of the reconstruction from the learned network's prediction, weights\n"
+           "    file as python -m feilab_b200.warmstart export writes it; the ICON phase ends at --tol, default 0.02,\n"
+           "    and every slice whose warm result fails the acceptance test is solved again from zero; the\n"
+           "    cross-validation solve always starts from zero)\n");
 }
 
 struct Args {
@@ -69,6 +74,7 @@ struct Args {
     double tol = 0.0;
     bool resume = false;
     int window = ICON_WINDOW_GAUSS6;
+    std::string warm;   // --warm-start weights file
 };
 
 // Per-GPU work: a contiguous slice range.
@@ -77,6 +83,7 @@ struct Job {
     int y0 = 0, y1 = 0;   // [y0, y1)
     int rc = 0;
     std::string err;
+    long long warm_accepted = 0, warm_redone = 0;
 };
 
 std::string join(const std::string &a, const std::string &b) { return a + "/" + b; }
@@ -175,6 +182,17 @@ void run_job(Job &job, const Args &A, const MrcHeader &inh, const std::vector<fl
         } destroy{plan};
         if (icon_plan_set_operator(plan, A.op) != ICON_OK || icon_plan_set_stop(plan, A.tol, 10) != ICON_OK)
             return fail("plan options");
+        // --warm-start: the network for this plan (destroyed before the plan).
+        struct Net {
+            icon_ws *w = nullptr;
+            ~Net() { icon_ws_destroy(w); }
+        } net;
+        if (!A.warm.empty()) {
+            icon_warm_cfg wc{A.tol > 0.0 ? A.tol : 0.02, 10, 2.0};
+            if (icon_ws_create(plan, std::min(cap, 32), &net.w) != ICON_OK || icon_ws_load(net.w, A.warm.c_str()) != ICON_OK ||
+                icon_plan_set_warm_start(plan, net.w, &wc) != ICON_OK)
+                return fail("warm start");
+        }
         std::vector<char> done(S, 0);
         if (A.resume) {
             // A finished slice: its file exists with this run's sizes; its
@@ -230,6 +248,7 @@ void run_job(Job &job, const Args &A, const MrcHeader &inh, const std::vector<fl
             }
             r0 = r1;
         }
+        if (net.w) icon_plan_warm_counts(plan, &job.warm_accepted, &job.warm_redone);
     }
     if (A.skip_cv) return;
     // Cross-validation solve without the smallest-|angle| tilt, reprojected
@@ -283,6 +302,7 @@ int main(int argc, char **argv)
             else if (a == "--tol" && next_arg(argc, argv, i, v)) A.tol = std::max(0.0, atof(v.c_str()));
             else if (a == "--operator" && next_arg(argc, argv, i, v) && (v == "nufft" || v == "toeplitz"))
                 A.op = v == "toeplitz" ? ICON_OPERATOR_TOEPLITZ : ICON_OPERATOR_NUFFT;
+            else if (a == "--warm-start" && next_arg(argc, argv, i, v)) A.warm = v;
             else if (a == "--window" && next_arg(argc, argv, i, v) && (v == "gauss6" || v == "kb4"))
                 A.window = v == "kb4" ? ICON_WINDOW_KB4 : ICON_WINDOW_GAUSS6;
             else if (a == "--help") { help(); return -1; }
@@ -441,6 +461,14 @@ int main(int argc, char **argv)
             printf("running state: fail!\nError message: %s\n", job.err.c_str());
             return 1;
         }
+    if (!A.warm.empty()) {
+        long long acc = 0, redo = 0;
+        for (auto &job : jobs) {
+            acc += job.warm_accepted;
+            redo += job.warm_redone;
+        }
+        printf("warm start: %lld of %lld slices accepted, %lld solved again from zero\n", acc, acc + redo, redo);
+    }
     if (!A.volume.empty()) {
         MrcHeader vh = inh;
         vh.nx = inh.nx;

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "icon_b200.h"
+#include "icon_warmstart.h"
 
 namespace iconx {
 
@@ -35,6 +36,9 @@ icon_status plan_iteration(icon_plan *p, int S, int it, const icon_solve_cfg *cf
 // After the last iteration: any deferred update, then m as [S][N0][N1]
 // (Y fastest) into d_out.
 icon_status plan_stage_out(icon_plan *p, int S, const icon_solve_cfg *cfg, float *d_out, cudaStream_t st);
+
+// Slices a warm-start network takes per call (icon_ws_create's capacity).
+int ws_capacity(const icon_ws *w);
 
 // Sets icon_last_error() and returns st.
 icon_status fail_msg(icon_status st, const std::string &msg);

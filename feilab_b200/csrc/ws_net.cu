@@ -20,12 +20,14 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
 #include <vector>
 
 #include "icon_b200.h"
+#include "icon_internal.h"
 #include "icon_warmstart.h"
 #include "ws_kernels.cuh"
 
@@ -345,9 +347,8 @@ icon_status icon_ws_create(icon_plan *plan, int capacity, icon_ws **out)
     int dims[10];
     NET_TRY(icon_plan_query(plan, dims));
     auto w = std::make_unique<icon_ws>();
-    int dev = 0;
-    NET_CUDA(cudaGetDevice(&dev));
-    w->dev = dev;
+    w->dev = iconx::plan_device(plan);
+    DevGuard dg(w->dev);
     w->N0 = dims[0];
     w->N1 = dims[1];
     if (capacity > dims[7]) return net_fail(ICON_ERR_CAPACITY, "warm-start capacity above the plan's");
@@ -467,6 +468,30 @@ icon_status icon_ws_set_gain(icon_ws *w, float gain)
     return ICON_OK;
 }
 
+icon_status icon_ws_load(icon_ws *w, const char *path)
+{
+    if (!w || !path) return net_fail(ICON_ERR_INVALID, "icon_ws_load: null argument");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return net_fail(ICON_ERR_IO, std::string("icon_ws_load: cannot open ") + path);
+    char magic[8];
+    unsigned long long count = 0;
+    float gain = 0.f;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "ICONWSB1", 8) == 0 &&
+              std::fread(&count, sizeof(count), 1, f) == 1 && std::fread(&gain, sizeof(gain), 1, f) == 1;
+    std::vector<float> p;
+    if (ok && count == w->nparam) {
+        p.resize(count);
+        ok = std::fread(p.data(), sizeof(float), count, f) == count;
+    } else {
+        ok = false;
+    }
+    std::fclose(f);
+    if (!ok)
+        return net_fail(ICON_ERR_IO, std::string("icon_ws_load: ") + path + " is not a weights file of " +
+                                         std::to_string(w->nparam) + " parameters");
+    return icon_ws_set_params(w, p.data(), p.size(), gain);
+}
+
 icon_status icon_ws_predict(icon_ws *w, const void *d_Ahwb, float *d_m0, int S, void *stream)
 {
     NET_TRY(check_ws(w, S));
@@ -540,3 +565,5 @@ icon_status icon_ws_get_grads(icon_ws *w, float *h_grads, size_t count)
 }
 
 }  // extern "C"
+
+int iconx::ws_capacity(const icon_ws *w) { return w ? w->cap : 0; }

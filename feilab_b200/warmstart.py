@@ -40,9 +40,12 @@ def lib():
         L.icon_ws_get_grads.argtypes = [P, V, Z]
         L.icon_ws_update.argtypes = [P, F, V]
         L.icon_ws_train_step.argtypes = [P, V, V, I, F, ctypes.POINTER(D), V]
+        L.icon_ws_load.argtypes = [P, ctypes.c_char_p]
+        L.icon_plan_set_warm_start.argtypes = [P, P, V]
+        L.icon_plan_warm_counts.argtypes = [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
         for name in ("icon_ws_create", "icon_ws_destroy", "icon_ws_init", "icon_ws_set_params", "icon_ws_get_params",
                      "icon_ws_set_gain", "icon_ws_predict", "icon_ws_backprop", "icon_ws_get_grads", "icon_ws_update",
-                     "icon_ws_train_step"):
+                     "icon_ws_train_step", "icon_ws_load", "icon_plan_set_warm_start", "icon_plan_warm_counts"):
             getattr(L, name).restype = ctypes.c_int
         _ws_ready = True
     return L
@@ -181,6 +184,10 @@ class Network:
     def update(self, lr):
         _check(lib().icon_ws_update(self._h, float(lr), _stream()))
 
+    def load(self, path):
+        """Parameters and gain from a weights file written by save_raw."""
+        _check(lib().icon_ws_load(self._h, str(path).encode()))
+
     def train_step(self, Ahwb, target, lr):
         S = self._in(Ahwb, target)
         loss = ctypes.c_double(0)
@@ -202,3 +209,45 @@ def load_weights(path=None, nx=1024, thickness=300):
     path = path or os.path.join(WEIGHTS_DIR, f"warmstart_{nx}x{thickness}.npz")
     z = np.load(path)
     return z["params"].astype(np.float32), float(z["gain"]), json.loads(str(z["meta"]))
+
+
+def save_raw(path, params, gain):
+    """The weights file icon_ws_load reads (icon-gpu --warm-start): the 8
+    bytes ICONWSB1, the parameter count (uint64), the gain (float32), then
+    the FP32 parameters, little-endian."""
+    import struct
+    import numpy as np
+    p = np.ascontiguousarray(np.asarray(params, "<f4"))
+    with open(path, "wb") as f:
+        f.write(b"ICONWSB1")
+        f.write(struct.pack("<Qf", p.size, float(gain)))
+        f.write(p.tobytes())
+
+
+def set_warm_start(plan, net, tol, check_every=10, max_dist=2.0):
+    """Warm start of the plan's reconstruct calls (icon_plan_set_warm_start);
+    net None turns it off."""
+    from .icon import WarmCfg
+    if net is None:
+        _check(lib().icon_plan_set_warm_start(plan._h, None, None))
+        return
+    wc = WarmCfg(float(tol), int(check_every), float(max_dist))
+    _check(lib().icon_plan_set_warm_start(plan._h, net._h, ctypes.byref(wc)))
+
+
+def warm_counts(plan):
+    """(accepted, redone from zero) slices of the plan's warm-started reconstruct calls."""
+    a, r = ctypes.c_longlong(0), ctypes.c_longlong(0)
+    _check(lib().icon_plan_warm_counts(plan._h, ctypes.byref(a), ctypes.byref(r)))
+    return int(a.value), int(r.value)
+
+
+if __name__ == "__main__":
+    # python -m feilab_b200.warmstart export WEIGHTS.npz OUT.bin
+    import sys
+    if len(sys.argv) == 4 and sys.argv[1] == "export":
+        prm, g, _ = load_weights(sys.argv[2])
+        save_raw(sys.argv[3], prm, g)
+    else:
+        print("usage: python -m feilab_b200.warmstart export WEIGHTS.npz OUT.bin")
+        sys.exit(2)

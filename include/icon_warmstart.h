@@ -82,6 +82,27 @@ icon_status icon_ws_update(icon_ws *ws, float lr, void *stream);
 icon_status icon_ws_train_step(icon_ws *ws, const void *d_Ahwb, const float *d_target, int S, float lr,
                                double *h_loss, void *stream);
 
+/* Loads parameters and output gain from a weights file: the 8 bytes
+ * "ICONWSB1", the parameter count (uint64, little-endian), the gain (float32)
+ * and the FP32 parameters (as written by feilab_b200.warmstart.save_raw from a
+ * trained network's .npz).  Fails with ICON_ERR_IO when the file does not
+ * hold this network's parameter count. */
+icon_status icon_ws_load(icon_ws *ws, const char *path);
+
+/* Warm start of the plan's reconstruct calls (icon_reconstruct_host,
+ * icon_reconstruct_stack, icon_reconstruct_stack_host): after the input
+ * stage, the network `ws` (made for this plan; it must outlive the use)
+ * predicts each slice's start and icon_solve_warm with `wc` solves from it,
+ * redoing from m = 0 every slice its acceptance test rejects.  ws = NULL
+ * turns it off (the reference's cold start, Iteration2.cu:33).  Allocates
+ * two image buffers of the plan's capacity on first use.  No counterpart in
+ * the reference. */
+icon_status icon_plan_set_warm_start(icon_plan *plan, icon_ws *ws, const icon_warm_cfg *wc);
+
+/* Slices the plan's warm-started reconstruct calls have accepted and redone
+ * from m = 0 since the plan was made. */
+icon_status icon_plan_warm_counts(const icon_plan *plan, long long *h_accepted, long long *h_redone);
+
 /* Test of the convolution's bounded waits (no reference counterpart): one
  * convolution as icon_ws_conv3x3 (one input, no bias, no ReLU, one output)
  * whose first pipeline stage waits for 16 bytes more than its loads deliver,

@@ -234,3 +234,35 @@ def test_cli_kaiser_bessel_window(golden, tmp_path):
         assert rel_l2(rk, r) < TOL_SOLVE, n
     p = _run(base + ["-skipCV", "1", "--window", "kb6"], str(tmp_path))
     assert p.returncode != 0 and "parameter error!" in p.stdout
+
+
+@pytest.mark.gpu
+def test_cli_warm_start(golden, tmp_path):
+    # --warm-start FILE: the shipped network's weights exported to the raw
+    # file format; every slice is either accepted from its warm start or
+    # solved again from zero, the counts are printed, and the slices stay
+    # finite and near the cold run's.  A file that is not a weights file is
+    # refused.
+    from feilab_b200 import mrc, warmstart
+    params, gain, _ = warmstart.load_weights()
+    wfile = tmp_path / "net.bin"
+    warmstart.save_raw(str(wfile), params, gain)
+    sched = (2, 40, 2)
+    z, out, base = _cli_case(golden, tmp_path, "cold", sched)
+    S = int(z["S"])
+    assert _run(base + ["-skipCV", "1"], str(tmp_path)).returncode == 0
+    _, out_w, base_w = _cli_case(golden, tmp_path, "warm", sched)
+    p = _run(base_w + ["-skipCV", "1", "--warm-start", str(wfile), "--tol", "0.05"], str(tmp_path))
+    assert p.returncode == 0, p.stdout + p.stderr
+    line = [ln for ln in p.stdout.splitlines() if ln.startswith("warm start:")]
+    assert line and f"of {S} slices accepted" in line[0], p.stdout
+    for s in range(S):
+        _, d = mrc.read(str(out / "reconstruction" / f"mid{s:05d}.mrc"))
+        _, dw = mrc.read(str(out_w / "reconstruction" / f"mid{s:05d}.mrc"))
+        assert np.all(np.isfinite(dw))
+        assert rel_l2(dw[0], d[0]) < 0.5, s
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(b"not weights")
+    _, out_b, base_b = _cli_case(golden, tmp_path, "bad", sched)
+    p = _run(base_b + ["-skipCV", "1", "--warm-start", str(bad)], str(tmp_path))
+    assert p.returncode != 0 and "warm start" in p.stdout

@@ -75,3 +75,38 @@ def test_invalid_acceptance_settings_are_rejected(case):
     for kw in ({"tol": 0.0}, {"tol": 0.05, "max_dist": 0.0}, {"tol": 0.05, "check_every": 0}):
         with pytest.raises(IconError):
             plan.solve_warm(A, m_cold.clone(), iters=SCHED, data_type=DTYPE, threshold=THR, **kw)
+
+
+def test_reconstruct_calls_with_warm_start(case):
+    # icon_plan_set_warm_start: the reconstruct calls start each slice from
+    # the network's prediction and use icon_solve_warm.  With every network
+    # parameter at zero the prediction is m0 = 0, so an accepted slice is the
+    # cold solve stopped at the tolerance and a redone one the full cold
+    # solve, bit for bit; the counts add up; turning it off restores the
+    # plain reconstruction.
+    import numpy as np
+    from feilab_b200 import icon, synth, warmstart
+    plan, A, m_cold = case
+    nx, th, S = plan.N0, plan.N1, A.shape[0]
+    tilts = synth.tilt_angles(-60, 60, 2)
+    ph = synth.make_phantom((nx, S, th), 60, seed=41)
+    rows = synth.add_noise(synth.project(ph, tilts), 0.5, 41).numpy().astype(np.float32)
+    net = warmstart.Network(plan, capacity=4)
+    net.set_params(np.zeros(net.n, np.float32), 1.0)
+    tol = 0.05
+    warmstart.set_warm_start(plan, net, tol)
+    got = plan.reconstruct_host(rows, SCHED, DTYPE, THR)
+    acc, redo = warmstart.warm_counts(plan)
+    assert acc + redo == S
+    m_tol, _, _ = plan.solve_until(A, tol, SCHED, DTYPE, THR)
+    m_tol = m_tol.cpu().numpy()
+    cold = m_cold.cpu().numpy()
+    got = got[0] if isinstance(got, tuple) else got
+    got = np.asarray(got)
+    for s in range(S):
+        assert np.array_equal(got[s], m_tol[s]) or np.array_equal(got[s], cold[s]), s
+    warmstart.set_warm_start(plan, None, tol)
+    plain = plan.reconstruct_host(rows, SCHED, DTYPE, THR)
+    plain = np.asarray(plain[0] if isinstance(plain, tuple) else plain)
+    assert np.array_equal(plain, cold)
+    net.close()
