@@ -277,7 +277,8 @@ struct icon_plan {
     long long warm_accepted = 0, warm_redone = 0;
     bool xt_tma = false, xt_tma_m = false;
     int xt_bh = 1, xt_box_g1 = 0, xt_box_img = 0;
-    CUtensorMap tm_g1, tm_ahwb, tm_rhat, tm_m;
+    CUtensorMap tm_g1, tm_ahwb, tm_rre, tm_m;
+    float *rre = nullptr;       // [Gcap][N1][N0][B] Re r-hat of the Toeplitz x-kernels (the deferred update's input)
     int *dev_err = nullptr;
     bool upd_pending = false, upd_clamp = false;
     int upd_dtype = 0, upd_G = 0;
@@ -360,7 +361,7 @@ struct icon_plan {
         if (xt_tma) {
             xa.tm_g1 = tm_g1;
             xa.tm_ahwb = tm_ahwb;
-            xa.tm_rhat = tm_rhat;
+            xa.tm_rre = tm_rre;
             xa.tm_m = tm_m;
         }
     }
@@ -481,14 +482,14 @@ void setup_xt_tma(icon_plan *p)
         const cuuint64_t str[2] = {Bz * 8, N0 * Bz * 8};
         const cuuint32_t box[3] = {(cuuint32_t)(BH * 2), (cuuint32_t)p->xt_box_img, 1};
         ok = ok && make_map(&p->tm_ahwb, p->Ahwb, 3, dims, str, box);
-        ok = ok && make_map(&p->tm_rhat, p->rhat, 3, dims, str, box);
+
     }
     bool ok_m = BH >= 4;
     if (ok_m) {   // m [Gcap N1][N0][B] floats
         const cuuint64_t dims[3] = {Bz, N0, G * N1};
         const cuuint64_t str[2] = {Bz * 4, N0 * Bz * 4};
         const cuuint32_t box[3] = {(cuuint32_t)BH, (cuuint32_t)p->xt_box_img, 1};
-        ok_m = make_map(&p->tm_m, p->m, 3, dims, str, box);
+        ok_m = make_map(&p->tm_m, p->m, 3, dims, str, box) && make_map(&p->tm_rre, p->rre, 3, dims, str, box);
     }
     p->xt_tma = ok;
     p->xt_tma_m = ok && ok_m;
@@ -746,9 +747,10 @@ icon_status flush_update(icon_plan *p, cudaStream_t st)
     const int G = p->upd_G;
     int per_group = p->N1 * p->N0 * p->B;
     dim3 gu((unsigned)std::min<size_t>(((size_t)per_group + 255) / 256, 512), G);
-    WITH_B(p->B, LAUNCH_B(p, K_UPD, st, stage_bytes(p, p->nodes).upd * G * p->B,
-                          L::update(gu, st, p->m, p->rhat, p->alpha, per_group, p->upd_clamp ? 1 : 0, p->upd_dtype,
-                                    p->upd_thr)))
+    // m read and written, Re r-hat read
+    WITH_B(p->B, LAUNCH_B(p, K_UPD, st, (double)p->N0 * p->N1 * 12 * G * p->B,
+                          L::update_re(gu, st, p->m, p->rre, p->alpha, per_group, p->upd_clamp ? 1 : 0, p->upd_dtype,
+                                       p->upd_thr)))
     ICON_CUDA(cudaGetLastError());
     return ICON_OK;
 }
@@ -771,14 +773,14 @@ icon_status launch_iteration_xt_raw(icon_plan *p, int G, bool upd, bool clamp_pr
     icon::XtArgs xa{};
     p->fill_xt(xa);
     xa.N0 = p->N0; xa.N1 = p->N1; xa.n0 = p->n0; xa.tw0 = p->tw0; xa.G1 = p->G1; xa.m = p->m;
-    xa.rhat_in = p->rhat; xa.alpha = p->alpha; xa.upd = upd ? 1 : 0; xa.clamp = clamp_prev ? 1 : 0;
-    xa.data_type = data_type; xa.thr = thr; xa.rhat = p->rhat; xa.Ahwb = p->Ahwb; xa.part_rtr = p->part_rtr;
-    const double xf_bytes = (xa.upd ? NN * 16 : NN * 4) + G1b;
+    xa.rre_in = p->rre; xa.alpha = p->alpha; xa.upd = upd ? 1 : 0; xa.clamp = clamp_prev ? 1 : 0;
+    xa.data_type = data_type; xa.thr = thr; xa.rre = p->rre; xa.Ahwb = p->Ahwb; xa.part_rtr = p->part_rtr;
+    const double xf_bytes = (xa.upd ? NN * 12 : NN * 4) + G1b;   // m (read, written), Re r-hat; G1 written
     dim3 gy(G, p->n0);
     WITH_B(p->B,
         LAUNCH_B(p, K_XTF, st, xf_bytes * slots, L::xtoep(0, st, G, xa));
         LAUNCH_B(p, K_YT, st, (2 * G1b) * slots + Kb * G, L::ypass_toep(p->ey, gy, p->thr_y, p->smem_yt, st, g, p->G1));
-        LAUNCH_B(p, K_XTM, st, (2 * G1b + NN * 16) * slots, L::xtoep(1, st, G, xa));
+        LAUNCH_B(p, K_XTM, st, (2 * G1b + NN * 12) * slots, L::xtoep(1, st, G, xa));
         LAUNCH_B(p, K_YQ, st, G1b * slots + Kb * G,
                  L::ypass_toep_quad(p->ey, gy, p->thr_y, p->smem_yt, st, g, p->G1, p->part_rtar)))
     LAUNCH(p, K_ALPHA, st, icon::k_alpha<<<G, 32 * p->B, 0, st>>>(p->part_rtr, p->N1, p->part_rtar, p->n0, p->B, p->alpha, hist_a, hist_r));
@@ -1135,6 +1137,7 @@ static icon_status plan_create_impl(const icon_geometry *geo, int group, icon_pl
     ICON_TRY(p->arena.alloc(&p->fline, G * p->nx * Bz));
     size_t NN = (size_t)p->N0 * p->N1;
     ICON_TRY(p->arena.alloc(&p->rhat, G * NN * Bz));
+    ICON_TRY(p->arena.alloc(&p->rre, G * NN * Bz));
     ICON_TRY(p->arena.alloc(&p->Ahwb, G * NN * Bz));
     ICON_TRY(p->arena.alloc(&p->imgc, G * NN * Bz));
     ICON_TRY(p->arena.alloc(&p->m, G * NN * Bz));

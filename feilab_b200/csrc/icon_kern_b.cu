@@ -216,6 +216,13 @@ void Launch<B>::update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat,
     else k_update<B, false><<<grid, 256, 0, st>>>(m, rhat, alpha, per_group, clamp, data_type, thr);
 }
 
+template <int B>
+void Launch<B>::update_re(dim3 grid, cudaStream_t st, float *m, const float *rre, const double *alpha, int per_group,
+                          int clamp, int data_type, float thr)
+{
+    k_update<B, false, float><<<grid, 256, 0, st>>>(m, rre, alpha, per_group, clamp, data_type, thr);
+}
+
 // The dynamic shared-memory limit is a property of the kernel function, not
 // of a plan: plans of different sizes share the variants of one B, so every
 // variant gets the device's opt-in maximum (what a launch actually asks for

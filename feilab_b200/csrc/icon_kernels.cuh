@@ -1024,18 +1024,22 @@ __global__ void k_step_reduce(const double *__restrict__ step_part, int nb, int 
 // m <- m - alpha*Re(rhat) computed in double and stored as float; ICON steps
 // also clamp (ICONUpdateCU_R NU:1597-1616, INFRUpdateCU_R NU:1630-1639).
 // m: [G][N1][N0][B] float, rhat: same layout float2.  blockIdx.y = group.
-template <int B, bool MEASURE = false>
-__global__ void k_update(float *__restrict__ m, const float2 *__restrict__ rhat, const double *__restrict__ alpha,
+__device__ __forceinline__ float re_part(float2 v) { return v.x; }
+__device__ __forceinline__ float re_part(float v) { return v; }
+
+// rhat: complex r-hat, or (RT = float) its real part alone.
+template <int B, bool MEASURE = false, typename RT = float2>
+__global__ void k_update(float *__restrict__ m, const RT *__restrict__ rhat, const double *__restrict__ alpha,
                          int per_group, int clamp, int data_type, float thr, double *__restrict__ step_part = nullptr)
 {
     const int grp = blockIdx.y;
     float *mg = m + (size_t)grp * per_group;
-    const float2 *rg = rhat + (size_t)grp * per_group;
+    const RT *rg = rhat + (size_t)grp * per_group;
     double dd = 0.0, mm = 0.0;   // MEASURE: sums of (m_new - m_old)^2 and m_new^2 of this thread's slot
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < per_group; i += gridDim.x * blockDim.x) {
         double a = alpha[grp * B + (i & (B - 1))];
         const float old = mg[i];
-        float v = (float)((double)old - a * (double)rg[i].x);
+        float v = (float)((double)old - a * (double)re_part(rg[i]));
         if (clamp) {
             if (data_type == 1) {
                 if (v > thr) v = thr;
@@ -1489,21 +1493,22 @@ struct XtArgs {
     const float2 *tw0;       // [n0] exp(-2 pi i q / n0)
     float2 *G1;              // [G][n0][N1][B]
     float *m;                // [G][N1][N0][B] real image (forward input; updated in place when upd)
-    const float2 *rhat_in;   // update: r-hat of the iteration being finished
+    const float *rre_in;     // update: Re r-hat of the iteration being finished, [G][N1][N0][B]
     const double *alpha;     // update: [G*B] step lengths
     int upd, clamp, data_type;
     float thr;
-    float2 *rhat;            // mid / adjoint: r-hat (or the adjoint) out, [G][N1][N0][B]
+    float2 *rhat;            // adjoint: the adjoint (or r-hat) out, [G][N1][N0][B]
+    float *rre;              // mid: Re r-hat out, [G][N1][N0][B] (the update needs only the real part)
     const float2 *Ahwb;      // mid / adjoint with resid: [G][N1][N0][B]
     double *part_rtr;        // mid / adjoint with resid: [G][N1][B] partial |r-hat|^2 per column
     const float *rcx, *rcy;  // adjoint: deapodisation reciprocals 1/cx [N0], 1/cy [N1]
     int resid;               // adjoint: subtract Ahwb and sum |.|^2 (else the plain adjoint)
     // TMA staging of the columns (use_tma; BH >= 2): the plan's G1 as 2-D
     // [Gcap n0 rows][N1 B 2 floats], its Ahwb and r-hat as 3-D
-    // [Gcap N1][N0][B 2 floats], and (tma_m; BH >= 4) its m as
-    // [Gcap N1][N0][B floats]; boxes of BH slices by box_g1 / box_img rows.
+    // [Gcap N1][N0][B 2 floats], and (tma_m; BH >= 4) its m and Re r-hat
+    // as [Gcap N1][N0][B floats]; boxes of BH slices by box_g1 / box_img rows.
     // Every wait on the loads is bounded and reports through err.
-    CUtensorMap tm_g1, tm_ahwb, tm_rhat, tm_m;
+    CUtensorMap tm_g1, tm_ahwb, tm_rre, tm_m;
     int use_tma, tma_m, box_g1, box_img;
     int *err;
 };
@@ -1761,26 +1766,27 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
         // The m column (N0 x BH floats) into s and, for the update, the r-hat
         // column into As, by cp.async; then into registers.
         float *Ms = reinterpret_cast<float *>(s);
+        float *Rs = reinterpret_cast<float *>(As);   // Re r-hat column, [N0][BH] floats
         if (tma && g.tma_m) {
-            // m and (for the update) the r-hat column by TMA, boxes of
-            // box_img points: m as [X][BH] floats into s, r-hat into As.
+            // m and (for the update) the Re r-hat column by TMA, boxes of
+            // box_img points: m as [X][BH] floats into s, Re r-hat into Rs.
             const int nbox = (N0 + g.box_img - 1) / g.box_img;
             if (t == 0) {
                 ws::mbar_expect_tx(&bar[0], (uint32_t)(nbox * g.box_img * BH * sizeof(float)));
                 for (int k = 0; k < nbox; ++k)
                     ws::tma_load_3d(Ms + k * g.box_img * BH, &g.tm_m, h * BH, k * g.box_img, grp * N1 + Y, &bar[0]);
                 if (g.upd) {
-                    ws::mbar_expect_tx(&bar[1], (uint32_t)(nbox * g.box_img * BH * sizeof(float2)));
+                    ws::mbar_expect_tx(&bar[1], (uint32_t)(nbox * g.box_img * BH * sizeof(float)));
                     for (int k = 0; k < nbox; ++k)
-                        ws::tma_load_3d(As + k * g.box_img * BH, &g.tm_rhat, h * BH * 2, k * g.box_img,
-                                        grp * N1 + Y, &bar[1]);
+                        ws::tma_load_3d(Rs + k * g.box_img * BH, &g.tm_rre, h * BH, k * g.box_img, grp * N1 + Y,
+                                        &bar[1]);
                 }
             }
             if (!xt_tma_wait(&bar[0], g.err)) return;
             if (g.upd && !xt_tma_wait(&bar[1], g.err)) return;
         } else {
             const float *msrc = g.m + ibase - sl;           // point X of this CTA's slices at msrc + X*B
-            const float2 *rsrc = g.rhat_in + ibase - sl;
+            const float *rsrc = g.rre_in + ibase - sl;
             for (int X = t; X < N0; X += S::T) {
                 if constexpr (BH == 4) cp_async<16>(Ms + X * 4, msrc + (size_t)X * B);
                 else if constexpr (BH == 2) cp_async<8>(Ms + X * 2, msrc + (size_t)X * B);
@@ -1791,11 +1797,14 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
                 }
             }
             if (g.upd) {
-                constexpr int P = BH >= 2 ? BH / 2 : 1;
-                for (int idx = t; idx < N0 * P; idx += S::T) {
-                    const int X = idx / P, c = idx - X * P;
-                    if constexpr (BH >= 2) cp_async<16>(As + X * BH + 2 * c, rsrc + (size_t)X * B + 2 * c);
-                    else cp_async<8>(As + X, rsrc + (size_t)X * B);
+                for (int X = t; X < N0; X += S::T) {
+                    if constexpr (BH == 4) cp_async<16>(Rs + X * 4, rsrc + (size_t)X * B);
+                    else if constexpr (BH == 2) cp_async<8>(Rs + X * 2, rsrc + (size_t)X * B);
+                    else if constexpr (BH == 1) cp_async<4>(Rs + X, rsrc + (size_t)X * B);
+                    else {
+                        cp_async<16>(Rs + X * BH, rsrc + (size_t)X * B);
+                        cp_async<16>(Rs + X * BH + 4, rsrc + (size_t)X * B + 4);
+                    }
                 }
             }
             cp_async_commit();
@@ -1809,7 +1818,7 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
             for (int idx = t; idx < N0 * BH; idx += S::T) {
                 const int X = idx / BH, q = idx - X * BH;
                 const double al = g.alpha[grp * B + h * BH + q];
-                float nv = (float)((double)Ms[idx] - al * (double)As[idx].x);
+                float nv = (float)((double)Ms[idx] - al * (double)Rs[idx]);
                 if (g.clamp) {
                     if (g.data_type == 1) {
                         if (nv > g.thr) nv = g.thr;
@@ -1906,7 +1915,7 @@ __global__ void __launch_bounds__(XtShape<BH, LA, LNB>::T, (XtShape<BH, LA, LNB>
                     const float2 av = As[X * BH + sl];
                     r = make_float2(v[i][a].x - av.x, v[i][a].y - av.y);
                     acc += (double)r.x * (double)r.x + (double)r.y * (double)r.y;
-                    g.rhat[ibase + (size_t)X * B] = r;
+                    g.rre[ibase + (size_t)X * B] = r.x;
                 }
                 v[i][a] = r;
             }

@@ -38,6 +38,9 @@ struct Launch {
                         const float2 *f, float *out, int S);
     static void update(dim3 grid, cudaStream_t st, float *m, const float2 *rhat, const double *alpha, int per_group,
                        int clamp, int data_type, float thr, double *step_part = nullptr);
+    // The same from the real part of r-hat alone (the Toeplitz x-kernels' output).
+    static void update_re(dim3 grid, cudaStream_t st, float *m, const float *rre, const double *alpha, int per_group,
+                          int clamp, int data_type, float thr);
     // Three-step x-passes (k_xtoep) over G groups: mode 0 the Toeplitz forward
     // of the real image (with the fused update when a.upd), mode 1 the
     // Toeplitz inverse, r-hat and forward of r-hat, mode 2 the NUFFT adjoint's
