@@ -495,6 +495,7 @@ def run_ours(args):
             "e2e": {"value": e2e, "unit": "slices/s", "h2d_bytes_per_step": int(S * len(tilts) * NX * 4),
                     "d2h_bytes_per_step": int(S * NX * THICK * 4)},
             "gpu_launches": int(head["launches"]),
+            "device_error": plan.device_error(),   # bounded TMA waits that ran out (0: none)
             "clocks": head["clocks"],
             "operators": {op: {"value": r["value"], "e2e": r["e2e"], "steps": r["steps"],
                                "ms_per_step": r["t"] / r["steps"] * 1e3,
