@@ -1349,6 +1349,11 @@ __global__ void __launch_bounds__(R * B, (R == 20 && B == 8) ? 4 : (512 / (R * B
     const int t = threadIdx.x, b = t & (B - 1), u = t >> LB;
     float2 *row = G1 + ((size_t)grp * g.n0 + x) * N1 * B;
     const float *krow = g.Kt + toep_kernel_index(g, grp) * g.kstride + (size_t)x * (32 * R);
+    // The twiddle table wn^q, q < 32 R, copied behind the transposed values;
+    // every twiddle of the two steps is read from it.
+    float2 *tws = s + 32 * R * B;
+    for (int q = t; q < 32 * R / 2; q += R * B) cp_async<16>(tws + 2 * q, g.tw1 + 2 * q);
+    cp_async_commit();
 
     // Step 1: R-point DFTs over a, twiddles wn^(c k1), transpose.
     {
@@ -1362,21 +1367,15 @@ __global__ void __launch_bounds__(R * B, (R == 20 && B == 8) ? 4 : (512 / (R * B
 #pragma unroll
             for (int a = 0; a < R; ++a) v[i][a] = a < na ? rb[32 * B * a] : make_float2(0.f, 0.f);
         }
+        cp_async_wait<0>();
+        __syncthreads();   // the twiddle table is in shared memory
 #pragma unroll
         for (int i = 0; i < NI; ++i) {
             const int c = u + R * i;
             if (c >= 32) break;
             dft_nat<R>(v[i], -1.f);
-            // wn^(c k1): from the table at k1 = 0, 8, 16, 24, stepped by
-            // wn^c in between (at most 7 products from a table value).
-            const float2 w1 = __ldg(&g.tw1[c]);
-            float2 tw = w1;
 #pragma unroll
-            for (int k1 = 1; k1 < R; ++k1) {
-                if ((k1 & 7) == 0) tw = __ldg(&g.tw1[c * k1]);
-                else if (k1 > 1) tw = cmul(tw, w1);
-                v[i][k1] = cmul(v[i][k1], tw);
-            }
+            for (int k1 = 1; k1 < R; ++k1) v[i][k1] = cmul(v[i][k1], tws[c * k1]);
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) s[ytoep4_sidx<B, R>(c, k1, b)] = v[i][k1];
         }
@@ -1416,21 +1415,11 @@ __global__ void __launch_bounds__(R * B, (R == 20 && B == 8) ? 4 : (512 / (R * B
             for (int j = 0; j < 4; ++j) w[4 * q + j] = make_float2(w[4 * q + j].x * kv[j], w[4 * q + j].y * kv[j]);
         }
         dft_dif_inplace<32>(w, +1.f);
-        {
-            // conj(wn^(c u)), table at c = 0, 8, 16, 24, products between.
-            float2 w1 = __ldg(&g.tw1[u]);
-            w1.y = -w1.y;
-            float2 tw = w1;
 #pragma unroll
-            for (int c = 1; c < 32; ++c) {
-                if ((c & 7) == 0) {
-                    tw = __ldg(&g.tw1[c * u]);
-                    tw.y = -tw.y;
-                } else if (c > 1) {
-                    tw = cmul(tw, w1);
-                }
-                w[brev5(c)] = cmul(w[brev5(c)], tw);
-            }
+        for (int c = 1; c < 32; ++c) {   // conj(wn^(c u)) from the table
+            float2 tw = tws[c * u];
+            tw.y = -tw.y;
+            w[brev5(c)] = cmul(w[brev5(c)], tw);
         }
         __syncthreads();   // every read of s is done before it is overwritten
 #pragma unroll
@@ -1454,7 +1443,7 @@ __global__ void __launch_bounds__(R * B, (R == 20 && B == 8) ? 4 : (512 / (R * B
     }
 }
 
-__host__ __device__ inline size_t ytoep4_smem(int n1, int B) { return (size_t)n1 * B * sizeof(float2); }
+__host__ __device__ inline size_t ytoep4_smem(int n1, int B) { return (size_t)n1 * (B + 1) * sizeof(float2); }
 // n1 sizes k_ytoep4 takes (n1 = 32 R, R in ytoep4_radix_ok).
 __host__ __device__ inline bool ytoep4_fits(int n1) { return n1 % 32 == 0 && ytoep4_radix_ok(n1 / 32); }
 
