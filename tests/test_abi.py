@@ -57,3 +57,23 @@ def test_shipped_warm_start_weights_match_the_network():
     params, gain, meta = warmstart.load_weights()
     assert params.size == warmstart.param_count()
     assert gain > 0 and meta["nx"] == 1024 and meta["thickness"] == 300
+
+
+def test_raw_weights_file_layout(tmp_path):
+    # The weights file icon-gpu --warm-start reads (icon_ws_load): magic,
+    # uint64 parameter count, float32 gain, then the FP32 parameters, for
+    # both shipped networks (1024x300 and the 512x256 one of the
+    # learned-start workload).
+    import struct
+    import numpy as np
+    from feilab_b200 import warmstart
+    for nx, th in ((1024, 300), (512, 256)):
+        params, gain, meta = warmstart.load_weights(nx=nx, thickness=th)
+        assert params.size == warmstart.param_count() and (meta["nx"], meta["thickness"]) == (nx, th)
+        f = tmp_path / f"w{nx}.bin"
+        warmstart.save_raw(str(f), params, gain)
+        raw = f.read_bytes()
+        assert raw[:8] == b"ICONWSB1"
+        n, g = struct.unpack("<Qf", raw[8:20])
+        assert n == params.size and abs(g - gain) <= 1e-6 * abs(gain)
+        assert np.array_equal(np.frombuffer(raw[20:], "<f4"), params)
